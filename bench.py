@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 state-vector engine.
+
+Workload (one "step"): the n=30, depth-40 random circuit — per layer U3 with U[0,2pi)
+angles on all 30 qubits, then 15 CX on a seeded random perfect matching (1,800 gates) —
+applied in FP64 to a 16 GiB state resident in HBM, through the staged engine.  The state
+(16 GiB) is far larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+Printed (rank 0, one JSON line): gates/s over all ranks, the roofline of the dominant
+kernel (the staged tile kernel, HBM-bound), the reference CPU path timed on this box's
+host cores, an end-to-end figure through the C ABI with host buffers, the SM clocks seen
+during the timed region, and secondary forms (per-gate FP64 sweeps, adjoint gradients).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank runs the same workload on its own GPU: a single circuit
+does not shard without an exchange step, so the multi-GPU figure is N replicas.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sv-sim_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+N_QUBITS = 30
+DEPTH = 40
+SEED = 2024
+METRIC = "n=30 gates/s & HBM GB/s: FP64 per-gate vs fused TC (1-F≤1e-6); adjoint grads/s"
+UNIT = "gates/s"
+WORKLOAD = "random circuit n=30 depth 40 (U3 all qubits + 15 CX random matching per layer), FP64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-extras", action="store_true", help="skip the secondary forms")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_sample_gates(circuit):
+    """The bounded CPU sample: every third gate of the first layer (15 of its 45 gates:
+    10 U3 spread over low and high qubits and 5 CX), applied to the 30-qubit state."""
+    return circuit[:45][::3].copy()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.reader.join(timeout=2)
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_rate(circuit, threads):
+    """gates/s of the reference's OpenMP CPU backend on the bounded sample."""
+    from oracle.oracle import RefBackend
+    sample = cpu_sample_gates(circuit)
+    kind, backend = "reference", None
+    for k in ("omp64",):
+        if RefBackend.available(k):
+            backend = RefBackend(k)
+    if backend is None:
+        return None
+    h = backend.open(N_QUBITS, threads)
+    try:
+        ms = backend.run_on(h, sample)
+    finally:
+        backend.close(h)
+    return {"value": len(sample) / (ms / 1e3), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{len(sample)} gates of layer 1 (every 3rd) at n=30, reference "
+                      f"svsim_cpu_omp.hpp (64-bit IdxType build), sim() wall time {ms:.0f} ms"}
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from svsim_b200 import circuits
+    from oracle.oracle import RefBackend
+    circuit = circuits.random_matching_circuit(N_QUBITS, DEPTH, seed=SEED)
+    threads = os.cpu_count() or 1
+    if not RefBackend.available("omp64"):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference CPU backend not built (oracle/_ref missing)"}))
+        return
+    sample = cpu_sample_gates(circuit)
+    backend = RefBackend("omp64")
+    h = backend.open(N_QUBITS, threads)
+    for _ in range(args.warmup):
+        backend.run_on(h, sample)
+    times = [backend.run_on(h, sample) for _ in range(args.steps)]
+    backend.close(h)
+    total_s = sum(times) / 1e3
+    value = len(sample) * args.steps / total_s
+    sample_desc = (f"{len(sample)} gates of layer 1 (every 3rd) at n=30 per step, reference "
+                   f"svsim_cpu_omp.hpp (64-bit IdxType build), {threads} threads")
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_qubits": N_QUBITS, "depth": DEPTH, "seed": SEED,
+                   "sample": sample_desc},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample_desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_ours(args):
+    import torch
+    from svsim_b200 import circuits, _native as nat
+
+    world, rank, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    device = local
+    torch.cuda.set_device(device)
+    circuit = circuits.random_matching_circuit(N_QUBITS, DEPTH, seed=SEED)
+    n_gates = len(circuit)
+
+    h = nat.Handle(N_QUBITS, device, nat.SVB_FP64)
+    h.set_engine(nat.ENGINE_STAGED, 12, 0)
+    h.set_circuit(circuit)
+    info = h.plan_info()
+    stream = torch.cuda.current_stream(device)
+    sptr = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(max(args.warmup, 3)):
+        h.run(sptr)
+    torch.cuda.synchronize(device)
+    barrier()
+    torch.cuda.synchronize(device)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            h.run(sptr)
+        ev1.record(stream)
+        torch.cuda.synchronize(device)
+    barrier()
+    torch.cuda.synchronize(device)
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * n_gates * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel: every staged pass reads and writes the state once
+    state_bytes = info.state_bytes
+    passes = int(info.n_passes)
+    per_launch_bytes = 2.0 * state_bytes
+    launch_s = (ms / 1e3) / (args.steps * passes)
+    achieved = per_launch_bytes / launch_s / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "staged_fp64_traffic.txt")
+    if os.path.exists(tfile):
+        for ln in open(tfile):
+            if ln.startswith("bytes_per_launch_n30"):
+                traffic = float(ln.split("=")[1])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "k_staged<double,12> (one read+write of the 16 GiB state per launch)",
+                "peak_source": f"{peak_kind} hbm_gbs",
+                "per_launch_bytes": per_launch_bytes, "launches_per_step": passes,
+                "gate_model_gbs": info.model_bytes / (ms_per_step / 1e3) / 1e9}
+
+    # end to end through the C ABI with host buffers: circuit upload + plan, run,
+    # 1024-shot measurement back to host
+    shots = 1024
+    uni = np.random.default_rng(0).random(shots)
+    pinned_gates = torch.from_numpy(circuit.view(np.uint8).copy()).pin_memory()
+    e2e_steps = max(2, min(args.steps, 3))
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        h.set_circuit(pinned_gates.numpy().view(circuit.dtype))
+        h.run(sptr)
+        samples, _tot = h.measure(uni)
+    torch.cuda.synchronize(device)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e = {"value": world * n_gates / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": int(circuit.nbytes + info.plan_bytes + uni.nbytes),
+           "d2h_bytes_per_step": int(samples.nbytes + 8),
+           "path": "svb_set_circuit + svb_run + svb_measure(1024 shots), host buffers"}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_qubits": N_QUBITS, "depth": DEPTH, "gates": n_gates,
+                   "seed": SEED, "engine": "staged", "tile_bits": int(info.tile_bits),
+                   "passes": passes, "parallelism": f"replicas x{world}",
+                   "l2": "16 GiB state > 126 MB L2: every step streams from HBM, no flush"},
+        "roofline": roofline,
+        "e2e": e2e,
+        "clocks": clocks.summary(),
+        "gpu_launches": int(args.steps * passes),
+    }
+    del h
+    torch.cuda.empty_cache()
+
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        try:
+            out["cpu_baseline"] = cpu_reference_rate(circuit, threads)
+        except Exception as e:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"value": None, "error": str(e)}
+    if rank == 0 and not args.no_extras and world == 1:
+        out["forms"] = secondary_forms(device, circuit)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def secondary_forms(device, circuit):
+    """Per-gate FP64 sweeps on the same circuit, and adjoint gradients (n=20, 480 params)."""
+    import torch
+    from svsim_b200 import circuits, _native as nat
+    forms = {}
+    # per-gate engine on the first 4 layers (180 gates): one kernel per elementary op
+    h = nat.Handle(N_QUBITS, device, nat.SVB_FP64)
+    h.set_engine(nat.ENGINE_PER_GATE, 0, 0)
+    sub = circuit[:180]
+    h.set_circuit(sub)
+    info = h.plan_info()
+    h.run()
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    h.run()
+    e1.record()
+    torch.cuda.synchronize(device)
+    s = e0.elapsed_time(e1) / 1e3
+    peak, _ = peaks()
+    forms["per_gate_fp64"] = {"gates_per_s": len(sub) / s, "hbm_gbs": info.moved_bytes / s / 1e9,
+                              "frac_of_peak": info.moved_bytes / s / 1e9 / peak,
+                              "sample": "first 4 layers (180 gates), one sweep per gate"}
+    del h
+    torch.cuda.empty_cache()
+    forms["fused_tc_fp32"] = None
+    # adjoint: n=20 hardware-efficient ansatz, 720 gates, 480 parameters
+    pc = circuits.hardware_efficient_ansatz()
+    terms = circuits.zz_x_hamiltonian(20)
+    ha = nat.Handle(20, device, nat.SVB_FP64)
+    ha.adjoint(pc.gates, pc.binding, 480, terms)
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ha.adjoint(pc.gates, pc.binding, 480, terms)
+    t_adj = (time.perf_counter() - t0) / reps
+    # parameter shift on the same GPU: 2 circuits per parameter (timed on 48 of 480)
+    hp = nat.Handle(20, device, nat.SVB_FP64)
+    nshift = 48
+    t0 = time.perf_counter()
+    for p in range(nshift):
+        for sgn in (1, -1):
+            pp = pc.params.copy()
+            pp[p] += sgn * math.pi / 2
+            hp.reset()
+            hp.set_circuit(pc.evaluated(pp))
+            hp.run()
+            hp.expectation(terms)
+    t_shift = (time.perf_counter() - t0) / nshift * 480
+    forms["adjoint"] = {"grads_per_s": 1.0 / t_adj, "param_shift_grads_per_s": 1.0 / t_shift,
+                        "speedup_vs_param_shift": t_shift / t_adj,
+                        "workload": "n=20, 12 layers RY+RZ+CX ring, 720 gates, P=480, "
+                                    "H = sum ZZ + 0.5 sum X",
+                        "param_shift_sample": f"{nshift} of 480 parameters timed, scaled"}
+    return forms
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

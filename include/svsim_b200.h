@@ -1,0 +1,191 @@
+/*
+ * svsim_b200.h — C ABI of the B200 state-vector engine (libsvsim_b200.so).
+ *
+ * This is the boundary that the reference's single-GPU backend
+ * (svsim/src/svsim_nvgpu_sin.cuh) crosses into hand-written sm_100a kernels.  The
+ * reference's C++ API (class Simulation / class Gate, and the pybind11 module built
+ * from svsim/src/py_wrapper.cpp) is kept as a header-only drop-in under
+ * include/svsim_dropin/, which calls these functions.  Every entry point below names
+ * the reference code it replaces.
+ *
+ * Conventions
+ *   - Plain C types only: host pointers, sizes, and an opaque `void* stream` that is a
+ *     cudaStream_t (NULL = the legacy default stream).
+ *   - Every function returns an svb_status; SVB_OK is 0.  On failure the reason is
+ *     available from svb_last_error() on the calling thread.  Nothing in the library
+ *     calls exit() or assert(): invalid gates, qubit indices and sizes are rejected
+ *     on the host before any kernel runs.
+ *   - Qubit q is bit q of the basis-state index (little-endian), as in the reference.
+ *   - A handle owns its device memory and is used from one host thread at a time.
+ */
+#ifndef SVSIM_B200_H
+#define SVSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum svb_status {
+    SVB_OK = 0,
+    SVB_ERR_INVALID = 1,      /* bad argument, gate, qubit index or size */
+    SVB_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    SVB_ERR_OOM = 3,          /* device or host allocation failed */
+    SVB_ERR_UNSUPPORTED = 4,  /* valid request this build does not support */
+    SVB_ERR_STATE = 5         /* call out of order (e.g. run before a circuit is set) */
+} svb_status;
+
+typedef enum svb_precision {
+    SVB_FP64 = 0,  /* complex<double> amplitudes: the reference's ValType (config.hpp:42) */
+    SVB_FP32 = 1   /* complex<float> amplitudes: fused tensor-core and batched forms */
+} svb_precision;
+
+typedef enum svb_engine {
+    SVB_ENGINE_AUTO = 0,      /* staged for n >= 10, per-gate below */
+    SVB_ENGINE_PER_GATE = 1,  /* one HBM sweep per elementary gate, as the reference */
+    SVB_ENGINE_STAGED = 2,    /* many gates per HBM sweep through a shared-memory tile */
+    SVB_ENGINE_FUSED = 3      /* gates fused into dense k-qubit blocks (FP32 only) */
+} svb_engine;
+
+/* One gate: the fields of the reference's class Gate (svsim_nvgpu_sin.cuh:99-188)
+ * without its device function pointer.  `op` is the reference's enum OP value
+ * (:42-48, U3 = 0 ... RYY = 37).  48 bytes. */
+typedef struct svb_gate {
+    uint32_t op;
+    uint32_t qb[5];
+    double theta, phi, lambda;
+} svb_gate;
+
+/* Parameter binding of one gate for the adjoint: for each angle field
+ * (0 = theta, 1 = phi, 2 = lambda) the index of the circuit parameter it depends on
+ * (-1 = constant) and d(angle)/d(parameter).  40 bytes. */
+typedef struct svb_param_binding {
+    int32_t idx[3];
+    int32_t reserved;
+    double coef[3];
+} svb_param_binding;
+
+/* One Pauli string of an observable: coef * prod_q sigma_q, where qubit q carries
+ * X if only x_mask has bit q, Z if only z_mask has it, Y if both do. */
+typedef struct svb_pauli_term {
+    double coef;
+    uint64_t x_mask;
+    uint64_t z_mask;
+} svb_pauli_term;
+
+/* Execution statistics of the current plan. */
+typedef struct svb_plan_info {
+    uint64_t n_gates;          /* gates as given */
+    uint64_t n_elementary;     /* elementary ops after expanding composites */
+    uint64_t n_passes;         /* kernel launches per run */
+    uint64_t n_sweeps_model;   /* per-gate sweep count of the reference (half sweeps x2) */
+    double   state_bytes;      /* bytes of the state vector */
+    double   model_bytes;      /* per-gate-model algorithmic bytes of one run */
+    double   moved_bytes;      /* bytes the plan reads+writes in HBM per run */
+    uint64_t plan_bytes;       /* bytes of plan descriptors uploaded by svb_set_circuit */
+    int      engine;           /* engine the plan was built for */
+    int      tile_bits;        /* local qubits per tile (staged engine) */
+} svb_plan_info;
+
+typedef struct svb_sim svb_sim;
+
+/* ---- lifetime ------------------------------------------------------------------- */
+
+/* Replaces Simulation::Simulation (svsim_nvgpu_sin.cuh:193-225): selects `device`,
+ * allocates the 2^n-amplitude state on it and sets |0..0>.  Unlike the reference no
+ * host copy of the state is kept.  n_qubits in [1, 36]. */
+svb_status svb_create(uint32_t n_qubits, int device, int precision, svb_sim** out);
+
+/* Replaces Simulation::~Simulation (:227-237). NULL is accepted. */
+svb_status svb_destroy(svb_sim* sim);
+
+/* Replaces Simulation::reset_sv (:243-255): state <- |0..0>, on the device. */
+svb_status svb_reset_state(svb_sim* sim);
+
+/* ---- circuit -------------------------------------------------------------------- */
+
+/* Replaces Simulation::append + Simulation::upload (:257-294): validates the gate list
+ * on the host (op in range, qubits < n, distinct qubits within a gate), expands the
+ * composites into the reference's elementary sequences (:1134-1454), plans the
+ * kernel passes and uploads the plan.  Replaces any previous circuit. */
+svb_status svb_set_circuit(svb_sim* sim, const svb_gate* gates, size_t n_gates);
+
+/* Replaces Simulation::clear_circuit (:341-358). The state is kept. */
+svb_status svb_clear_circuit(svb_sim* sim);
+
+/* Chooses the execution engine (svb_engine) for the next svb_set_circuit; tile_bits
+ * (0 = automatic) and fusion_width (0 = automatic, else 2..6) tune the staged and
+ * fused engines. */
+svb_status svb_set_engine(svb_sim* sim, int engine, int tile_bits, int fusion_width);
+
+/* Statistics of the current plan. */
+svb_status svb_get_plan_info(const svb_sim* sim, svb_plan_info* out);
+
+/* ---- execution ------------------------------------------------------------------ */
+
+/* Replaces Simulation::sim (:306-339) minus its full-state device-to-host copy:
+ * applies the current circuit to the device state, asynchronously on `stream`. */
+svb_status svb_run(svb_sim* sim, void* stream);
+
+/* Blocks until all work of this handle's device is done; reports kernel errors. */
+svb_status svb_synchronize(svb_sim* sim);
+
+/* ---- state access --------------------------------------------------------------- */
+
+/* The device-to-host copy at the end of Simulation::sim (:328-329): writes the state
+ * as the reference's SoA host arrays sv_real_cpu / sv_imag_cpu (2^n doubles each;
+ * FP32 states are widened).  Either pointer may be NULL. */
+svb_status svb_get_state_soa(svb_sim* sim, double* re, double* im);
+
+/* Loads an SoA host state (for tests and restarts; no reference counterpart). */
+svb_status svb_set_state_soa(svb_sim* sim, const double* re, const double* im);
+
+/* Device address of the interleaved (re, im) amplitude array and its precision. */
+svb_status svb_state_device_ptr(svb_sim* sim, void** dptr, int* precision);
+
+/* ---- measurement ---------------------------------------------------------------- */
+
+/* Replaces Simulation::measure (:359-383) with the uniforms supplied by the caller
+ * instead of rand(): shot s returns the j with S_j <= uniforms[s] < S_{j+1}, where
+ * S is the inclusive prefix sum of |amplitude|^2 in index order, and 0 if there is
+ * no such j — the reference's rule, including its default of 0.  The prefix sums
+ * are FP64 and computed on the GPU (hierarchically, no 2^n scan array).
+ * prob_total (may be NULL) receives S_{2^n}, the squared norm. */
+svb_status svb_measure(svb_sim* sim, const double* uniforms, uint32_t shots,
+                       uint64_t* out, double* prob_total);
+
+/* Squared norm sum |a|^2 in FP64 (the value the reference checks against 1 at :379). */
+svb_status svb_norm2(svb_sim* sim, double* out);
+
+/* Re <psi| sum_t coef_t P_t |psi> in FP64 for a Pauli-sum observable. */
+svb_status svb_expectation(svb_sim* sim, const svb_pauli_term* terms, size_t n_terms,
+                           double* out);
+
+/* ---- differentiation (no reference counterpart) --------------------------------- */
+
+/* Adjoint differentiation of E(p) = <psi(p)| H |psi(p)>, psi(p) = U(p)|0..0>:
+ * runs the circuit forward from |0..0>, forms lambda = H psi, then walks the
+ * elementary ops backwards applying U^dagger to psi and lambda while accumulating
+ * grad[binding.idx] += 2 Re <lambda| dU/dp |psi_prev> * binding.coef in FP64.
+ * `gates` carry the angle values at the current parameters; `bindings` (one per gate)
+ * say which angles depend on which of the n_params parameters.  Writes energy (may
+ * be NULL) and grad[n_params].  The handle's state is left holding psi(p). */
+svb_status svb_adjoint(svb_sim* sim, const svb_gate* gates, const svb_param_binding* bindings,
+                       size_t n_gates, uint32_t n_params, const svb_pauli_term* terms,
+                       size_t n_terms, double* energy, double* grad);
+
+/* ---- diagnostics ---------------------------------------------------------------- */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* svb_last_error(void);
+
+/* Library version string. */
+const char* svb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SVSIM_B200_H */

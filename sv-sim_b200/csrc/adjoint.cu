@@ -1,0 +1,449 @@
+// Adjoint differentiation (no counterpart in the reference).
+//
+// E(p) = <psi| H |psi>, psi = U_K ... U_1 |0..0>, U_k the elementary ops of the
+// circuit (the reference's composite sequences, lower.cpp).  After the forward pass
+// lambda = H psi.  Walking k = K..1:
+//     psi    <- U_k^dagger psi            (psi is now the state before op k)
+//     g[k,i] =  Re <lambda| dU_k/d ang_i |psi>
+//     lambda <- U_k^dagger lambda
+// and dE/dp = 2 sum_{k,i,f} g[k,i] * d ang_i / d field_f * d field_f / d p.
+// Only psi and lambda are held; to bound the drift of the reverse-propagated psi the
+// forward pass stores checkpoints, and psi is reloaded from them on the way back.
+// Every reduction is FP64 with a fixed order (per-block partials, then one pass).
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+#include <string>
+
+#include "gate_math.cuh"
+
+namespace svb {
+
+enum { EK_CONST = 0, EK_U3 = 1, EK_U2 = 2, EK_U1 = 3, EK_RX = 4, EK_RY = 5, EK_R = 6 };
+
+namespace {
+
+constexpr int ADJ_BLOCKS = 296;   // 2 x 148 SMs
+constexpr int ADJ_THREADS = 256;
+
+struct DMats {
+    double d[3][8];   // up to three derivative matrices, C1 layout
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
+    return s;
+}
+
+// One reverse step of a single-qubit elementary op (inverse applied as F_C1/F_DIAG).
+__global__ void __launch_bounds__(ADJ_THREADS)
+k_adj_step(double2* __restrict__ psi, double2* __restrict__ lam, uint64_t half, int q, int form,
+           Coef<double> inv, int nd, DMats dm, double* __restrict__ partial)
+{
+    __shared__ double red[ADJ_THREADS / 32];
+    double acc[3] = {0.0, 0.0, 0.0};
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t qd = 1ull << q;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < half; i += stride) {
+        const uint64_t p0 = insert_zero(i, q), p1 = p0 | qd;
+        double2 s0 = psi[p0], s1 = psi[p1];
+        double2 l0 = lam[p0], l1 = lam[p1];
+        if (form == F_DIAG) {
+            diag_zero<double>(F_DIAG, inv, s0);
+            diag_one<double>(F_DIAG, inv, s1);
+        } else {
+            dense_pair<double>(F_C1, inv, s0, s1);
+        }
+        for (int d = 0; d < nd; d++) {
+            const double* m = dm.d[d];
+            const double u0r = m[0] * s0.x - m[1] * s0.y + m[2] * s1.x - m[3] * s1.y;
+            const double u0i = m[0] * s0.y + m[1] * s0.x + m[2] * s1.y + m[3] * s1.x;
+            const double u1r = m[4] * s0.x - m[5] * s0.y + m[6] * s1.x - m[7] * s1.y;
+            const double u1i = m[4] * s0.y + m[5] * s0.x + m[6] * s1.y + m[7] * s1.x;
+            acc[d] += l0.x * u0r + l0.y * u0i + l1.x * u1r + l1.y * u1i;
+        }
+        if (form == F_DIAG) {
+            diag_zero<double>(F_DIAG, inv, l0);
+            diag_one<double>(F_DIAG, inv, l1);
+        } else {
+            dense_pair<double>(F_C1, inv, l0, l1);
+        }
+        psi[p0] = s0; psi[p1] = s1;
+        lam[p0] = l0; lam[p1] = l1;
+    }
+    for (int d = 0; d < nd; d++) {
+        const double s = block_sum(acc[d], red);
+        if (threadIdx.x == 0) partial[(size_t)d * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS)
+k_adj_cx(double2* __restrict__ psi, double2* __restrict__ lam, uint64_t quarter, int c, int t)
+{
+    const int lo = c < t ? c : t, hi = c < t ? t : c;
+    const uint64_t cd = 1ull << c, td = 1ull << t;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < quarter; i += stride) {
+        const uint64_t b = insert_zero(insert_zero(i, lo), hi);
+        const uint64_t p0 = b | cd, p1 = b | cd | td;
+        const double2 a0 = psi[p0], a1 = psi[p1];
+        psi[p0] = a1; psi[p1] = a0;
+        const double2 b0 = lam[p0], b1 = lam[p1];
+        lam[p0] = b1; lam[p1] = b0;
+    }
+}
+
+// out = sum_t coef_t P_t psi
+__global__ void __launch_bounds__(256)
+k_pauli_apply(const double2* __restrict__ psi, double2* __restrict__ out, uint64_t dim,
+              const svb_pauli_term* __restrict__ terms, int n_terms)
+{
+    extern __shared__ svb_pauli_term sterms[];
+    for (int t = threadIdx.x; t < n_terms; t += blockDim.x) sterms[t] = terms[t];
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += stride) {
+        double accr = 0.0, acci = 0.0;
+        for (int t = 0; t < n_terms; t++) {
+            const uint64_t j = i ^ sterms[t].x_mask;
+            const double2 b = psi[j];
+            double br = b.x, bi = b.y;
+            if (__popcll(j & sterms[t].z_mask) & 1) { br = -br; bi = -bi; }
+            double tr, ti;
+            switch (__popcll(sterms[t].x_mask & sterms[t].z_mask) & 3) {
+            case 0: tr = br; ti = bi; break;
+            case 1: tr = -bi; ti = br; break;
+            case 2: tr = -br; ti = -bi; break;
+            default: tr = bi; ti = -br; break;
+            }
+            accr += sterms[t].coef * tr;
+            acci += sterms[t].coef * ti;
+        }
+        out[i] = make_double2(accr, acci);
+    }
+}
+
+__global__ void __launch_bounds__(256)
+k_inner_re(const double2* __restrict__ a, const double2* __restrict__ b, uint64_t dim,
+           double* __restrict__ partial)
+{
+    __shared__ double red[8];
+    double acc = 0.0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += stride) {
+        const double2 x = a[i], y = b[i];
+        acc += x.x * y.x + x.y * y.y;
+    }
+    const double s = block_sum(acc, red);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// results[r] = sum of partial[r * nblocks .. +nblocks), one warp per result
+__global__ void k_reduce_rows(const double* __restrict__ partial, int nblocks, int rows,
+                              double* __restrict__ results)
+{
+    const int lane = threadIdx.x & 31;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (row >= rows) return;
+    double s = 0.0;
+    for (int i = lane; i < nblocks; i += 32) s += partial[(size_t)row * nblocks + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) results[row] = s;
+}
+
+unsigned adj_grid(uint64_t items)
+{
+    const uint64_t need = (items + ADJ_THREADS - 1) / ADJ_THREADS;
+    return (unsigned)std::min<uint64_t>(std::max<uint64_t>(need, 1), ADJ_BLOCKS);
+}
+
+// d M / d ang_i for the elementary kinds, C1 layout.  Returns false if the op has no
+// derivative with respect to ang_i.
+bool deriv_matrix(const EOp& e, int i, double* m)
+{
+    std::memset(m, 0, 8 * sizeof(double));
+    const double S2I = 0.70710678118654752440;
+    switch (e.kind) {
+    case EK_U3: {
+        const double th = e.ang[0], ph = e.ang[1], la = e.ang[2];
+        const double c = std::cos(th / 2), s = std::sin(th / 2);
+        if (i == 0) {
+            m[0] = -0.5 * s;
+            m[2] = -0.5 * std::cos(la) * c; m[3] = -0.5 * std::sin(la) * c;
+            m[4] = 0.5 * std::cos(ph) * c;  m[5] = 0.5 * std::sin(ph) * c;
+            m[6] = -0.5 * std::cos(ph + la) * s; m[7] = -0.5 * std::sin(ph + la) * s;
+        } else if (i == 1) {
+            m[4] = -std::sin(ph) * s; m[5] = std::cos(ph) * s;
+            m[6] = -std::sin(ph + la) * c; m[7] = std::cos(ph + la) * c;
+        } else {
+            m[2] = std::sin(la) * s; m[3] = -std::cos(la) * s;
+            m[6] = -std::sin(ph + la) * c; m[7] = std::cos(ph + la) * c;
+        }
+        return true;
+    }
+    case EK_U2: {
+        const double ph = e.ang[1], la = e.ang[2];
+        if (i == 1) {
+            m[4] = -S2I * std::sin(ph); m[5] = S2I * std::cos(ph);
+            m[6] = -S2I * std::sin(ph + la); m[7] = S2I * std::cos(ph + la);
+            return true;
+        }
+        if (i == 2) {
+            m[2] = S2I * std::sin(la); m[3] = -S2I * std::cos(la);
+            m[6] = -S2I * std::sin(ph + la); m[7] = S2I * std::cos(ph + la);
+            return true;
+        }
+        return false;
+    }
+    case EK_U1:
+        if (i != 2) return false;
+        m[6] = -std::sin(e.ang[2]);
+        m[7] = std::cos(e.ang[2]);
+        return true;
+    case EK_RX: {
+        if (i != 0) return false;
+        const double c = std::cos(e.ang[0] / 2), s = std::sin(e.ang[0] / 2);
+        m[0] = -0.5 * s; m[3] = -0.5 * c; m[5] = -0.5 * c; m[6] = -0.5 * s;
+        return true;
+    }
+    case EK_RY: {
+        if (i != 0) return false;
+        const double c = std::cos(e.ang[0] / 2), s = std::sin(e.ang[0] / 2);
+        m[0] = -0.5 * s; m[2] = -0.5 * c; m[4] = 0.5 * c; m[6] = -0.5 * s;
+        return true;
+    }
+    default:
+        return false;
+    }
+}
+
+// U^dagger of an elementary op as an F_C1 / F_DIAG / F_CX op.
+bool inverse_op(const EOp& e, EOp& inv)
+{
+    inv = e;
+    const double S2I = 0.70710678118654752440;
+    double* m = inv.m;
+    auto c1 = [&](double a, double b, double c, double d, double e_, double f, double g, double h) {
+        inv.form = F_C1;
+        m[0] = a; m[1] = b; m[2] = c; m[3] = d; m[4] = e_; m[5] = f; m[6] = g; m[7] = h;
+    };
+    auto dg = [&](double a, double b, double c, double d) {
+        inv.form = F_DIAG;
+        std::memset(m, 0, 8 * sizeof(double));
+        m[0] = a; m[1] = b; m[2] = c; m[3] = d;
+    };
+    switch (e.form) {
+    case F_C1: c1(e.m[0], -e.m[1], e.m[4], -e.m[5], e.m[2], -e.m[3], e.m[6], -e.m[7]); return true;
+    case F_X:  c1(0, 0, 1, 0, 1, 0, 0, 0); return true;
+    case F_Y:  c1(0, 0, 0, -1, 0, 1, 0, 0); return true;
+    case F_H:  c1(S2I, 0, S2I, 0, S2I, 0, -S2I, 0); return true;
+    case F_W:  c1(S2I, 0, 0, S2I, 0, S2I, S2I, 0); return true;
+    case F_RX: c1(e.m[0], 0, 0, e.m[1], 0, e.m[1], e.m[0], 0); return true;   // RX(-theta)
+    case F_RY: c1(e.m[0], 0, e.m[2], 0, e.m[1], 0, e.m[3], 0); return true;   // transpose
+    case F_Z:  dg(1, 0, -1, 0); return true;
+    case F_S:  dg(1, 0, 0, -1); return true;
+    case F_SDG: dg(1, 0, 0, 1); return true;
+    case F_T:  dg(1, 0, S2I, -S2I); return true;
+    case F_TDG: dg(1, 0, S2I, S2I); return true;
+    case F_U1: dg(1, 0, e.m[0], -e.m[1]); return true;
+    case F_DIAG: dg(e.m[0], -e.m[1], e.m[2], -e.m[3]); return true;
+    case F_CX: return true;
+    default: return false;   // F_R, F_SRN: not unitary
+    }
+}
+
+}  // namespace
+
+}  // namespace svb
+
+using namespace svb;
+
+extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_param_binding* bindings,
+                                  size_t n_gates, uint32_t n_params, const svb_pauli_term* terms,
+                                  size_t n_terms, double* energy, double* grad)
+{
+    if (!s) { set_error("svb_adjoint: NULL handle"); return SVB_ERR_INVALID; }
+    if ((n_gates && (!gates || !bindings)) || (n_terms && !terms) || (n_params && !grad)) {
+        set_error("svb_adjoint: NULL argument");
+        return SVB_ERR_INVALID;
+    }
+    if (s->precision != SVB_FP64) {
+        set_error("svb_adjoint: the adjoint runs on FP64 states");
+        return SVB_ERR_UNSUPPORTED;
+    }
+    if (n_terms > 4096) { set_error("svb_adjoint: at most 4096 terms"); return SVB_ERR_INVALID; }
+    for (size_t t = 0; t < n_terms; t++)
+        if ((terms[t].x_mask | terms[t].z_mask) >> s->n) {
+            set_error("svb_adjoint: observable acts on a qubit >= n_qubits");
+            return SVB_ERR_INVALID;
+        }
+    for (size_t i = 0; i < n_gates; i++)
+        for (int f = 0; f < 3; f++)
+            if (bindings[i].idx[f] >= (int32_t)n_params) {
+                set_error("svb_adjoint: binding of gate " + std::to_string(i) + " names parameter " +
+                          std::to_string(bindings[i].idx[f]) + " >= n_params");
+                return SVB_ERR_INVALID;
+            }
+    // validates the gates, builds the forward plan and replaces the circuit
+    svb_status rc = svb_set_circuit(s, gates, n_gates);
+    if (rc != SVB_OK) return rc;
+    const int n = (int)s->n;
+    const uint64_t dim = 1ull << n;
+    const std::vector<EOp> eops = s->eops;
+    const size_t K = eops.size();
+
+    // derivative slots
+    struct Slot { size_t k; int i; };
+    std::vector<Slot> slots;
+    std::vector<int> first_slot(K, -1), n_slot(K, 0);
+    for (size_t k = 0; k < K; k++) {
+        const EOp& e = eops[k];
+        const svb_param_binding& b = bindings[e.gate];
+        for (int i = 0; i < 3; i++) {
+            bool used = false;
+            for (int f = 0; f < 3; f++)
+                if (b.idx[f] >= 0 && e.jac[i][f] != 0.0) used = true;
+            if (!used) continue;
+            if (e.kind == EK_R || e.kind == EK_CONST) {
+                set_error("svb_adjoint: gate " + std::to_string(e.gate) + " has a bound angle on a "
+                          "non-differentiable op (R is not unitary)");
+                return SVB_ERR_UNSUPPORTED;
+            }
+            if (first_slot[k] < 0) first_slot[k] = (int)slots.size();
+            slots.push_back({k, i});
+            n_slot[k]++;
+        }
+        EOp inv;
+        if (!inverse_op(e, inv)) {
+            set_error("svb_adjoint: gate " + std::to_string(e.gate) + " is not unitary (R or SRN)");
+            return SVB_ERR_UNSUPPORTED;
+        }
+    }
+
+    cudaError_t err = cudaSuccess;
+    double2* lam = nullptr;
+    double* partial = nullptr;
+    double* results = nullptr;
+    svb_pauli_term* dterms = nullptr;
+    std::vector<void*> ckpts;
+    std::vector<size_t> ckpt_at;   // op index where checkpoint c was taken (state before op)
+    auto cleanup = [&]() {
+        cudaFree(lam); cudaFree(partial); cudaFree(results); cudaFree(dterms);
+        for (void* p : ckpts) cudaFree(p);
+        lam = nullptr; partial = nullptr; results = nullptr; dterms = nullptr;
+        ckpts.clear();
+    };
+    auto fail = [&](cudaError_t e, const char* what) {
+        cleanup();
+        set_error(std::string("svb_adjoint: ") + what + ": " + cudaGetErrorString(e));
+        (void)cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? SVB_ERR_OOM : SVB_ERR_CUDA;
+    };
+    const size_t sbytes = dim * sizeof(double2);
+    if ((err = cudaMalloc(&lam, sbytes)) != cudaSuccess) return fail(err, "cudaMalloc(lambda)");
+    const size_t nslots = std::max<size_t>(slots.size(), 1);
+    if ((err = cudaMalloc(&partial, (nslots + 1) * ADJ_BLOCKS * sizeof(double))) != cudaSuccess)
+        return fail(err, "cudaMalloc(partials)");
+    if ((err = cudaMalloc(&results, (nslots + 1) * sizeof(double))) != cudaSuccess)
+        return fail(err, "cudaMalloc(results)");
+    if (n_terms && (err = cudaMalloc(&dterms, n_terms * sizeof(svb_pauli_term))) != cudaSuccess)
+        return fail(err, "cudaMalloc(terms)");
+    if (n_terms && (err = cudaMemcpy(dterms, terms, n_terms * sizeof(svb_pauli_term),
+                                     cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(err, "terms upload");
+
+    // checkpoints: up to 4 evenly spaced, if they fit in a quarter of free memory
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    int n_ck = (int)std::min<size_t>(4, free_b / 4 / sbytes);
+    if (K < 64) n_ck = 0;
+    for (int c = 0; c < n_ck; c++) {
+        void* p = nullptr;
+        if ((err = cudaMalloc(&p, sbytes)) != cudaSuccess) { (void)cudaGetLastError(); break; }
+        ckpts.push_back(p);
+        ckpt_at.push_back(K * (size_t)(c + 1) / (size_t)(n_ck + 1));
+    }
+
+    // forward, segment by segment
+    if ((err = launch_reset<double>(s->state, n, nullptr)) != cudaSuccess) return fail(err, "reset");
+    size_t begin = 0;
+    for (size_t c = 0; c <= ckpts.size(); c++) {
+        const size_t end = c < ckpts.size() ? ckpt_at[c] : K;
+        std::vector<EOp> seg(eops.begin() + begin, eops.begin() + end);
+        svb_status r2 = run_eops_staged(n, s->state, seg, nullptr);
+        if (r2 != SVB_OK) { cleanup(); return r2; }
+        if (c < ckpts.size() &&
+            (err = cudaMemcpyAsync(ckpts[c], s->state, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
+            return fail(err, "checkpoint");
+        begin = end;
+    }
+    // lambda = H psi, energy = Re <psi|lambda>
+    const unsigned g = adj_grid(dim);
+    if (n_terms)
+        k_pauli_apply<<<g, 256, n_terms * sizeof(svb_pauli_term)>>>(
+            static_cast<const double2*>(s->state), lam, dim, dterms, (int)n_terms);
+    else
+        err = cudaMemset(lam, 0, sbytes);
+    k_inner_re<<<ADJ_BLOCKS, 256>>>(static_cast<const double2*>(s->state), lam, dim,
+                                     partial + slots.size() * ADJ_BLOCKS);
+    k_reduce_rows<<<1, 32>>>(partial + slots.size() * ADJ_BLOCKS, ADJ_BLOCKS, 1, results + slots.size());
+    if ((err = cudaGetLastError()) != cudaSuccess) return fail(err, "energy");
+
+    // reverse sweep
+    double2* psi = static_cast<double2*>(s->state);
+    int ck = (int)ckpts.size() - 1;
+    const unsigned gp = adj_grid(dim / 2);
+    for (size_t kk = K; kk-- > 0;) {
+        const EOp& e = eops[kk];
+        EOp inv;
+        inverse_op(e, inv);
+        if (inv.form == F_CX) {
+            k_adj_cx<<<adj_grid(dim / 4), ADJ_THREADS>>>(psi, lam, dim / 4, (int)e.c, (int)e.q);
+        } else {
+            DMats dm;
+            std::memset(&dm, 0, sizeof(dm));
+            const int nd = n_slot[kk];
+            for (int d = 0; d < nd; d++) deriv_matrix(e, slots[first_slot[kk] + d].i, dm.d[d]);
+            Coef<double> ci;
+            for (int j = 0; j < 8; j++) ci.m[j] = inv.m[j];
+            double* part = nd ? partial + (size_t)first_slot[kk] * ADJ_BLOCKS : partial;
+            k_adj_step<<<gp, ADJ_THREADS>>>(psi, lam, dim / 2, (int)e.q, inv.form, ci, nd, dm, part);
+        }
+        if ((err = cudaGetLastError()) != cudaSuccess) return fail(err, "reverse step");
+        // psi is now the state before op kk; reload the stored copy if there is one
+        if (ck >= 0 && ckpt_at[ck] == kk) {
+            if ((err = cudaMemcpyAsync(psi, ckpts[ck], sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
+                return fail(err, "checkpoint reload");
+            ck--;
+        }
+    }
+    if (!slots.empty())
+        k_reduce_rows<<<(unsigned)((slots.size() * 32 + 255) / 256), 256>>>(partial, ADJ_BLOCKS,
+                                                                          (int)slots.size(), results);
+    std::vector<double> host(slots.size() + 1);
+    if ((err = cudaMemcpy(host.data(), results, host.size() * sizeof(double), cudaMemcpyDeviceToHost)) !=
+        cudaSuccess)
+        return fail(err, "results download");
+    if (energy) *energy = host[slots.size()];
+    for (uint32_t p = 0; p < n_params; p++) grad[p] = 0.0;
+    for (size_t r = 0; r < slots.size(); r++) {
+        const EOp& e = eops[slots[r].k];
+        const svb_param_binding& b = bindings[e.gate];
+        for (int f = 0; f < 3; f++)
+            if (b.idx[f] >= 0 && e.jac[slots[r].i][f] != 0.0)
+                grad[b.idx[f]] += 2.0 * host[r] * e.jac[slots[r].i][f] * b.coef[f];
+    }
+    // leave psi(p) in the handle: rerun the forward plan
+    cleanup();
+    if ((err = launch_reset<double>(s->state, n, nullptr)) != cudaSuccess) return fail(err, "reset");
+    return svb_run(s, nullptr);
+}

@@ -1,0 +1,555 @@
+// C ABI of libsvsim_b200 (declared in include/svsim_b200.h).
+//
+// Host-side runtime of the engine: argument validation (the reference asserts or
+// exits instead, svsim_nvgpu_sin.cuh:259-264, util_nvgpu.cuh:29-65), lowering and
+// planning of the circuit, plan upload, launch sequencing (optionally replayed from a
+// CUDA graph), state transfer and measurement.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <algorithm>
+#include <string>
+
+#include "svb_internal.h"
+
+namespace svb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
+svb_status cuda_fail(cudaError_t e, const char* what)
+{
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    set_error(m);
+    (void)cudaGetLastError();   // clear a sticky launch error where possible
+    return e == cudaErrorMemoryAllocation ? SVB_ERR_OOM : SVB_ERR_CUDA;
+}
+
+#define SVB_CUDA(call, what)                                   \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what);     \
+    } while (0)
+
+svb_status invalid(const std::string& msg)
+{
+    set_error(msg);
+    return SVB_ERR_INVALID;
+}
+
+template <typename F>
+cudaError_t dispatch_prec(int precision, F&& f)
+{
+    if (precision == SVB_FP64) return f(double(0));
+    return f(float(0));
+}
+
+int n_qubit_slots(uint32_t op)
+{
+    static const int slots[38] = {
+        1, 1, 1, 2, 1, 1, 1, 1, 1, 1,
+        1, 1, 1, 1, 1, 1, 2, 2, 2, 2,
+        3, 3, 2, 2, 2, 2, 2, 2, 2, 3,
+        4, 4, 4, 5, 1, 1, 1, 2};
+    return op < 38 ? slots[op] : 0;
+}
+
+void free_plan(Sim* s)
+{
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
+    cudaFree(s->dplan.passes);
+    cudaFree(s->dplan.stages);
+    cudaFree(s->dplan.ops);
+    s->dplan = DevPlanBuffers{};
+    s->staged = StagedPlan{};
+    s->eops.clear();
+    s->gates.clear();
+    s->have_circuit = false;
+    std::memset(&s->info, 0, sizeof(s->info));
+}
+
+void free_scratch(Sim* s)
+{
+    cudaFree(s->mscr.block_sums);
+    cudaFree(s->mscr.block_prefix);
+    cudaFree(s->mscr.uniforms);
+    cudaFree(s->mscr.samples);
+    cudaFree(s->mscr.partial);
+    s->mscr = MeasureScratch{};
+}
+
+svb_status ensure_scratch(Sim* s, size_t shots)
+{
+    const size_t nb = measure_scratch_doubles((int)s->n);
+    if (s->mscr.cap_blocks < nb) {
+        cudaFree(s->mscr.block_sums);
+        cudaFree(s->mscr.block_prefix);
+        s->mscr.block_sums = s->mscr.block_prefix = nullptr;
+        s->mscr.cap_blocks = 0;
+        SVB_CUDA(cudaMalloc(&s->mscr.block_sums, nb * sizeof(double)), "cudaMalloc(block sums)");
+        SVB_CUDA(cudaMalloc(&s->mscr.block_prefix, (nb + 1) * sizeof(double)),
+                 "cudaMalloc(block prefix)");
+        s->mscr.cap_blocks = nb;
+    }
+    if (s->mscr.cap_shots < shots) {
+        cudaFree(s->mscr.uniforms);
+        cudaFree(s->mscr.samples);
+        s->mscr.uniforms = nullptr;
+        s->mscr.samples = nullptr;
+        s->mscr.cap_shots = 0;
+        SVB_CUDA(cudaMalloc(&s->mscr.uniforms, shots * sizeof(double)), "cudaMalloc(uniforms)");
+        SVB_CUDA(cudaMalloc(&s->mscr.samples, shots * sizeof(uint64_t)), "cudaMalloc(samples)");
+        s->mscr.cap_shots = shots;
+    }
+    if (s->mscr.cap_partial < (size_t)REDUCE_BLOCKS) {
+        SVB_CUDA(cudaMalloc(&s->mscr.partial, REDUCE_BLOCKS * sizeof(double)), "cudaMalloc(partials)");
+        s->mscr.cap_partial = REDUCE_BLOCKS;
+    }
+    return SVB_OK;
+}
+
+int pick_tile_bits(const Sim* s)
+{
+    const int n = (int)s->n;
+    if (s->tile_bits_req > 0) return s->tile_bits_req;
+    if (s->precision == SVB_FP64) {
+        if (n >= 20) return 12;
+        if (n >= 12) return 10;
+        return n;                 // 10 or 11: a single tile
+    }
+    if (n >= 20) return 13;
+    if (n >= 13) return 11;
+    return n;
+}
+
+bool staged_supported(int precision, int M)
+{
+    if (precision == SVB_FP64) return M >= 10 && M <= 12;
+    return M >= 11 && M <= 13;
+}
+
+svb_status launch_all(Sim* s, cudaStream_t st)
+{
+    const int n = (int)s->n;
+    if (s->engine == SVB_ENGINE_STAGED) {
+        for (size_t p = 0; p < s->staged.passes.size(); p++) {
+            cudaError_t e = dispatch_prec(s->precision, [&](auto t) {
+                using T = decltype(t);
+                return launch_staged_pass<T>(s->state, n, s->staged.M, (int)p, s->dplan, st);
+            });
+            if (e != cudaSuccess) return cuda_fail(e, "staged pass launch");
+        }
+    } else {
+        for (const EOp& op : s->eops) {
+            cudaError_t e = dispatch_prec(s->precision, [&](auto t) {
+                using T = decltype(t);
+                return launch_eop<T>(s->state, n, op, st);
+            });
+            if (e != cudaSuccess) return cuda_fail(e, "gate launch");
+        }
+    }
+    return SVB_OK;
+}
+
+bool use_graph(const Sim* s)
+{
+    static const bool disabled = std::getenv("SVB_NO_GRAPH") != nullptr;
+    if (disabled) return false;
+    return s->info.n_passes >= 4;
+}
+
+}  // namespace
+
+svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st)
+{
+    const int M = n >= 20 ? 12 : (n >= 12 ? 10 : n);
+    if (M < 10) {
+        for (const EOp& op : ops) {
+            cudaError_t e = launch_eop<double>(state, n, op, st);
+            if (e != cudaSuccess) return cuda_fail(e, "gate launch");
+        }
+        return SVB_OK;
+    }
+    StagedPlan P;
+    plan_staged(ops, n, M, 3, P);
+    if (P.passes.empty()) return SVB_OK;
+    DevPlanBuffers b;
+    cudaError_t e = cudaMalloc(&b.passes, P.passes.size() * sizeof(DevPass));
+    if (e == cudaSuccess) e = cudaMalloc(&b.stages, std::max<size_t>(1, P.stages.size()) * sizeof(DevStage));
+    if (e == cudaSuccess) e = cudaMalloc(&b.ops, std::max<size_t>(1, P.ops.size()) * sizeof(DevOp));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b.passes, P.passes.data(), P.passes.size() * sizeof(DevPass), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !P.stages.empty())
+        e = cudaMemcpy(b.stages, P.stages.data(), P.stages.size() * sizeof(DevStage), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !P.ops.empty())
+        e = cudaMemcpy(b.ops, P.ops.data(), P.ops.size() * sizeof(DevOp), cudaMemcpyHostToDevice);
+    for (size_t p = 0; e == cudaSuccess && p < P.passes.size(); p++)
+        e = launch_staged_pass<double>(state, n, M, (int)p, b, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(b.passes);
+    cudaFree(b.stages);
+    cudaFree(b.ops);
+    if (e != cudaSuccess) return cuda_fail(e, "staged run");
+    return SVB_OK;
+}
+
+}  // namespace svb
+
+using namespace svb;
+
+extern "C" {
+
+const char* svb_last_error(void) { return g_last_error.c_str(); }
+
+const char* svb_version(void) { return "svsim_b200 0.1 (sm_100a)"; }
+
+svb_status svb_create(uint32_t n_qubits, int device, int precision, svb_sim** out)
+{
+    if (!out) return invalid("svb_create: out is NULL");
+    *out = nullptr;
+    if (n_qubits < 1 || n_qubits > 36) return invalid("svb_create: n_qubits must be in [1, 36]");
+    if (precision != SVB_FP64 && precision != SVB_FP32)
+        return invalid("svb_create: precision must be SVB_FP64 or SVB_FP32");
+    int count = 0;
+    SVB_CUDA(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (device < 0 || device >= count) return invalid("svb_create: no such CUDA device");
+    SVB_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    svb_sim* s = new svb_sim();
+    s->n = n_qubits;
+    s->device = device;
+    s->precision = precision;
+    s->amp_bytes = precision == SVB_FP64 ? 16 : 8;
+    const size_t bytes = s->amp_bytes << n_qubits;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    if (bytes > free_b) {
+        delete s;
+        set_error("svb_create: state of " + std::to_string(bytes) + " bytes exceeds free device memory");
+        return SVB_ERR_OOM;
+    }
+    cudaError_t e = cudaMalloc(&s->state, bytes);
+    if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaMalloc(state)"); }
+    e = cudaMalloc(&s->d_small, 64 * sizeof(double));
+    if (e != cudaSuccess) { cudaFree(s->state); delete s; return cuda_fail(e, "cudaMalloc"); }
+    e = dispatch_prec(precision, [&](auto t) {
+        using T = decltype(t);
+        return launch_reset<T>(s->state, (int)n_qubits, nullptr);
+    });
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        cudaFree(s->state); cudaFree(s->d_small); delete s;
+        return cuda_fail(e, "reset");
+    }
+    *out = s;
+    return SVB_OK;
+}
+
+svb_status svb_destroy(svb_sim* s)
+{
+    if (!s) return SVB_OK;
+    cudaSetDevice(s->device);
+    free_plan(s);
+    free_scratch(s);
+    cudaFree(s->state);
+    cudaFree(s->d_small);
+    if (s->capture_stream) cudaStreamDestroy(s->capture_stream);
+    delete s;
+    return SVB_OK;
+}
+
+svb_status svb_reset_state(svb_sim* s)
+{
+    if (!s) return invalid("svb_reset_state: NULL handle");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    cudaError_t e = dispatch_prec(s->precision, [&](auto t) {
+        using T = decltype(t);
+        return launch_reset<T>(s->state, (int)s->n, nullptr);
+    });
+    if (e != cudaSuccess) return cuda_fail(e, "reset");
+    return SVB_OK;
+}
+
+svb_status svb_set_engine(svb_sim* s, int engine, int tile_bits, int fusion_width)
+{
+    if (!s) return invalid("svb_set_engine: NULL handle");
+    if (engine < SVB_ENGINE_AUTO || engine > SVB_ENGINE_FUSED)
+        return invalid("svb_set_engine: unknown engine");
+    if (engine == SVB_ENGINE_FUSED && s->precision != SVB_FP32)
+        return invalid("svb_set_engine: the fused engine runs FP32 states");
+    if (tile_bits != 0 && !staged_supported(s->precision, tile_bits))
+        return invalid("svb_set_engine: tile_bits must be 10..12 (FP64) or 11..13 (FP32)");
+    if (fusion_width != 0 && (fusion_width < 2 || fusion_width > 6))
+        return invalid("svb_set_engine: fusion_width must be 2..6");
+    s->engine_req = engine;
+    s->tile_bits_req = tile_bits;
+    s->fusion_req = fusion_width;
+    return SVB_OK;
+}
+
+svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
+{
+    if (!s) return invalid("svb_set_circuit: NULL handle");
+    if (n_gates > 0 && !gates) return invalid("svb_set_circuit: gates is NULL");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    // validate everything before touching the current plan
+    for (size_t i = 0; i < n_gates; i++) {
+        const svb_gate& g = gates[i];
+        const int k = n_qubit_slots(g.op);
+        if (k == 0) return invalid("gate " + std::to_string(i) + ": unknown op " + std::to_string(g.op));
+        // the reference asserts qb0..qb4 < n_qubits for every gate (:259-264)
+        for (int j = 0; j < 5; j++)
+            if (g.qb[j] >= s->n)
+                return invalid("gate " + std::to_string(i) + ": qubit index " +
+                               std::to_string(g.qb[j]) + " >= n_qubits");
+        for (int a = 0; a < k; a++)
+            for (int b = a + 1; b < k; b++)
+                if (g.qb[a] == g.qb[b])
+                    return invalid("gate " + std::to_string(i) + ": repeated qubit " +
+                                   std::to_string(g.qb[a]));
+    }
+    std::vector<EOp> eops;
+    eops.reserve(n_gates * 2);
+    double sweeps = 0;
+    for (size_t i = 0; i < n_gates; i++) {
+        lower_gate(gates[i], (int32_t)i, eops);
+        sweeps += reference_sweeps(gates[i].op);
+    }
+    free_plan(s);
+    s->gates.assign(gates, gates + n_gates);
+    s->eops.swap(eops);
+
+    int engine = s->engine_req;
+    const int n = (int)s->n;
+    const int M = pick_tile_bits(s);
+    if (engine == SVB_ENGINE_AUTO)
+        engine = (staged_supported(s->precision, M) && n >= M) ? SVB_ENGINE_STAGED : SVB_ENGINE_PER_GATE;
+    if (engine == SVB_ENGINE_FUSED) {
+        set_error("svb_set_circuit: the fused engine is not available in this build");
+        return SVB_ERR_UNSUPPORTED;
+    }
+    if (engine == SVB_ENGINE_STAGED && !(staged_supported(s->precision, M) && n >= M)) {
+        set_error("svb_set_circuit: the staged engine needs n_qubits >= tile bits (10 FP64, 11 FP32)");
+        return SVB_ERR_UNSUPPORTED;
+    }
+    s->engine = engine;
+
+    const double sb = (double)s->amp_bytes * (double)(1ull << n);
+    s->info.n_gates = n_gates;
+    s->info.n_elementary = s->eops.size();
+    s->info.n_sweeps_model = (uint64_t)(sweeps * 2 + 0.5) / 2;
+    s->info.state_bytes = sb;
+    s->info.model_bytes = 2.0 * sb * sweeps;
+    s->info.engine = engine;
+    if (engine == SVB_ENGINE_STAGED) {
+        const int G = s->precision == SVB_FP64 ? 3 : 4;
+        plan_staged(s->eops, n, M, G, s->staged);
+        const StagedPlan& P = s->staged;
+        SVB_CUDA(cudaMalloc(&s->dplan.passes, std::max<size_t>(1, P.passes.size()) * sizeof(DevPass)),
+                 "cudaMalloc(plan)");
+        SVB_CUDA(cudaMalloc(&s->dplan.stages, std::max<size_t>(1, P.stages.size()) * sizeof(DevStage)),
+                 "cudaMalloc(plan)");
+        SVB_CUDA(cudaMalloc(&s->dplan.ops, std::max<size_t>(1, P.ops.size()) * sizeof(DevOp)),
+                 "cudaMalloc(plan)");
+        if (!P.passes.empty())
+            SVB_CUDA(cudaMemcpy(s->dplan.passes, P.passes.data(), P.passes.size() * sizeof(DevPass),
+                                cudaMemcpyHostToDevice), "plan upload");
+        if (!P.stages.empty())
+            SVB_CUDA(cudaMemcpy(s->dplan.stages, P.stages.data(), P.stages.size() * sizeof(DevStage),
+                                cudaMemcpyHostToDevice), "plan upload");
+        if (!P.ops.empty())
+            SVB_CUDA(cudaMemcpy(s->dplan.ops, P.ops.data(), P.ops.size() * sizeof(DevOp),
+                                cudaMemcpyHostToDevice), "plan upload");
+        s->info.n_passes = P.passes.size();
+        s->info.tile_bits = M;
+        s->info.plan_bytes = P.passes.size() * sizeof(DevPass) + P.stages.size() * sizeof(DevStage) +
+                             P.ops.size() * sizeof(DevOp);
+        s->info.moved_bytes = 2.0 * sb * (double)P.passes.size();
+    } else {
+        s->info.n_passes = s->eops.size();
+        s->info.tile_bits = 0;
+        double moved = 0;
+        for (const EOp& e : s->eops)
+            moved += (e.form == F_CX) ? 0.5 * sb : (form_is_diag(e.form) && e.form != F_DIAG) ? sb : 2.0 * sb;
+        s->info.moved_bytes = moved;
+    }
+    s->have_circuit = true;
+    return SVB_OK;
+}
+
+svb_status svb_clear_circuit(svb_sim* s)
+{
+    if (!s) return invalid("svb_clear_circuit: NULL handle");
+    cudaSetDevice(s->device);
+    free_plan(s);
+    return SVB_OK;
+}
+
+svb_status svb_get_plan_info(const svb_sim* s, svb_plan_info* out)
+{
+    if (!s || !out) return invalid("svb_get_plan_info: NULL argument");
+    *out = s->info;
+    return SVB_OK;
+}
+
+svb_status svb_run(svb_sim* s, void* stream)
+{
+    if (!s) return invalid("svb_run: NULL handle");
+    if (!s->have_circuit) {
+        set_error("svb_run: no circuit set");
+        return SVB_ERR_STATE;
+    }
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (s->info.n_passes == 0) return SVB_OK;
+    if (use_graph(s)) {
+        if (!s->graph) {
+            if (!s->capture_stream)
+                SVB_CUDA(cudaStreamCreateWithFlags(&s->capture_stream, cudaStreamNonBlocking),
+                         "cudaStreamCreate");
+            SVB_CUDA(cudaStreamBeginCapture(s->capture_stream, cudaStreamCaptureModeThreadLocal),
+                     "cudaStreamBeginCapture");
+            svb_status rc = launch_all(s, s->capture_stream);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(s->capture_stream, &g);
+            if (rc != SVB_OK) { if (g) cudaGraphDestroy(g); return rc; }
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&s->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) { s->graph = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
+        }
+        SVB_CUDA(cudaGraphLaunch(s->graph, st), "cudaGraphLaunch");
+        return SVB_OK;
+    }
+    return launch_all(s, st);
+}
+
+svb_status svb_synchronize(svb_sim* s)
+{
+    if (!s) return invalid("svb_synchronize: NULL handle");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    SVB_CUDA(cudaDeviceSynchronize(), "kernel execution");
+    return SVB_OK;
+}
+
+svb_status svb_get_state_soa(svb_sim* s, double* re, double* im)
+{
+    if (!s) return invalid("svb_get_state_soa: NULL handle");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    const uint64_t dim = 1ull << s->n;
+    const uint64_t chunk = std::min<uint64_t>(dim, 1ull << 24);
+    double *dre = nullptr, *dim_ = nullptr;
+    SVB_CUDA(cudaMalloc(&dre, chunk * sizeof(double)), "cudaMalloc(staging)");
+    cudaError_t e = cudaMalloc(&dim_, chunk * sizeof(double));
+    if (e != cudaSuccess) { cudaFree(dre); return cuda_fail(e, "cudaMalloc(staging)"); }
+    for (uint64_t f = 0; f < dim && e == cudaSuccess; f += chunk) {
+        const uint64_t c = std::min(chunk, dim - f);
+        e = dispatch_prec(s->precision, [&](auto t) {
+            using T = decltype(t);
+            return launch_soa_split<T>(s->state, f, c, re ? dre : nullptr, im ? dim_ : nullptr, nullptr);
+        });
+        if (e == cudaSuccess && re) e = cudaMemcpy(re + f, dre, c * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && im) e = cudaMemcpy(im + f, dim_, c * sizeof(double), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(dre);
+    cudaFree(dim_);
+    if (e != cudaSuccess) return cuda_fail(e, "svb_get_state_soa");
+    return SVB_OK;
+}
+
+svb_status svb_set_state_soa(svb_sim* s, const double* re, const double* im)
+{
+    if (!s || !re || !im) return invalid("svb_set_state_soa: NULL argument");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    const uint64_t dim = 1ull << s->n;
+    const uint64_t chunk = std::min<uint64_t>(dim, 1ull << 24);
+    double *dre = nullptr, *dim_ = nullptr;
+    SVB_CUDA(cudaMalloc(&dre, chunk * sizeof(double)), "cudaMalloc(staging)");
+    cudaError_t e = cudaMalloc(&dim_, chunk * sizeof(double));
+    if (e != cudaSuccess) { cudaFree(dre); return cuda_fail(e, "cudaMalloc(staging)"); }
+    for (uint64_t f = 0; f < dim && e == cudaSuccess; f += chunk) {
+        const uint64_t c = std::min(chunk, dim - f);
+        e = cudaMemcpy(dre, re + f, c * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(dim_, im + f, c * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = dispatch_prec(s->precision, [&](auto t) {
+                using T = decltype(t);
+                return launch_soa_merge<T>(s->state, f, c, dre, dim_, nullptr);
+            });
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    }
+    cudaFree(dre);
+    cudaFree(dim_);
+    if (e != cudaSuccess) return cuda_fail(e, "svb_set_state_soa");
+    return SVB_OK;
+}
+
+svb_status svb_state_device_ptr(svb_sim* s, void** dptr, int* precision)
+{
+    if (!s || !dptr) return invalid("svb_state_device_ptr: NULL argument");
+    *dptr = s->state;
+    if (precision) *precision = s->precision;
+    return SVB_OK;
+}
+
+svb_status svb_measure(svb_sim* s, const double* uniforms, uint32_t shots, uint64_t* out,
+                       double* prob_total)
+{
+    if (!s) return invalid("svb_measure: NULL handle");
+    if (shots > 0 && (!uniforms || !out)) return invalid("svb_measure: NULL uniforms or output");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    svb_status rc = ensure_scratch(s, std::max<uint32_t>(shots, 1));
+    if (rc != SVB_OK) return rc;
+    if (shots > 0)
+        SVB_CUDA(cudaMemcpy(s->mscr.uniforms, uniforms, shots * sizeof(double), cudaMemcpyHostToDevice),
+                 "uniforms upload");
+    cudaError_t e = dispatch_prec(s->precision, [&](auto t) {
+        using T = decltype(t);
+        return measure_device<T>(s->state, (int)s->n, s->mscr.uniforms, shots, s->mscr.samples,
+                                 s->d_small, s->mscr, nullptr);
+    });
+    if (e != cudaSuccess) return cuda_fail(e, "measure");
+    if (shots > 0)
+        SVB_CUDA(cudaMemcpy(out, s->mscr.samples, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost),
+                 "samples download");
+    double total = 0;
+    SVB_CUDA(cudaMemcpy(&total, s->d_small, sizeof(double), cudaMemcpyDeviceToHost), "total download");
+    if (prob_total) *prob_total = total;
+    return SVB_OK;
+}
+
+svb_status svb_norm2(svb_sim* s, double* out)
+{
+    if (!out) return invalid("svb_norm2: NULL output");
+    return svb_measure(s, nullptr, 0, nullptr, out);
+}
+
+svb_status svb_expectation(svb_sim* s, const svb_pauli_term* terms, size_t n_terms, double* out)
+{
+    if (!s || !out || (n_terms > 0 && !terms)) return invalid("svb_expectation: NULL argument");
+    if (n_terms > 4096) return invalid("svb_expectation: at most 4096 terms");
+    for (size_t t = 0; t < n_terms; t++)
+        if ((terms[t].x_mask | terms[t].z_mask) >> s->n)
+            return invalid("svb_expectation: term acts on a qubit >= n_qubits");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    if (n_terms == 0) { *out = 0; return SVB_OK; }
+    svb_status rc = ensure_scratch(s, 1);
+    if (rc != SVB_OK) return rc;
+    svb_pauli_term* dterms = nullptr;
+    SVB_CUDA(cudaMalloc(&dterms, n_terms * sizeof(svb_pauli_term)), "cudaMalloc(terms)");
+    cudaError_t e = cudaMemcpy(dterms, terms, n_terms * sizeof(svb_pauli_term), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = dispatch_prec(s->precision, [&](auto t) {
+            using T = decltype(t);
+            return expectation_device<T>(s->state, (int)s->n, dterms, (int)n_terms, s->d_small,
+                                         s->mscr.partial, nullptr);
+        });
+    if (e == cudaSuccess) e = cudaMemcpy(out, s->d_small, sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dterms);
+    if (e != cudaSuccess) return cuda_fail(e, "svb_expectation");
+    return SVB_OK;
+}
+
+}  // extern "C"

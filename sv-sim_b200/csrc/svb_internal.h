@@ -1,0 +1,205 @@
+// Internal declarations of libsvsim_b200: elementary ops, the pass planner's output,
+// the device-side descriptors and the handle.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "svsim_b200.h"
+
+namespace svb {
+
+// ---------------------------------------------------------------------------------
+// Elementary ops.  The reference applies every gate as a sequence of these
+// (svsim_nvgpu_sin.cuh:654-1454); each form keeps the reference's arithmetic.
+// ---------------------------------------------------------------------------------
+enum Form : uint8_t {
+    F_C1 = 0,   // C1_GATE :654      general 2x2: m = e0r e0i e1r e1i e2r e2i e3r e3i
+    F_X,        // X_GATE :818
+    F_Y,        // Y_GATE :837
+    F_H,        // H_GATE :873
+    F_SRN,      // SRN_GATE :894
+    F_W,        // W_GATE :1428
+    F_RX,       // RX_GATE :1085     m[0] = cos(t/2), m[1] = -sin(t/2)
+    F_RY,       // RY_GATE :1104     m[0..3] = e0r e1r e2r e3r
+    // forms that only change the |1> amplitude of the pair (diagonal): the qubit
+    // need not be local to a tile
+    F_Z,        // Z_GATE :857
+    F_S,        // S_GATE :940
+    F_SDG,      // SDG_GATE :955
+    F_T,        // T_GATE :970
+    F_TDG,      // TDG_GATE :985
+    F_R,        // R_GATE :924       m[0] = phase
+    F_U1,       // U1_GATE :1022     m[0] = cos(l), m[1] = sin(l)
+    F_DIAG,     // diag(d0, d1), m = d0r d0i d1r d1i (adjoint inverses only)
+    // two-qubit
+    F_CX,       // CX_GATE :779      swap (c=1,t=0) <-> (c=1,t=1)
+    F_COUNT
+};
+
+__host__ __device__ inline bool form_is_diag(int f) { return f >= F_Z && f <= F_DIAG; }
+
+struct EOp {
+    uint8_t form = F_C1;
+    uint32_t q = 0;        // target (dense, CX) or the qubit of a diagonal op
+    uint32_t c = 0;        // control (CX)
+    double m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // --- adjoint bookkeeping ---
+    int32_t gate = -1;     // index of the source gate
+    uint8_t kind = 0;      // elementary kind for derivatives: see lower.cpp (EK_*)
+    double ang[3] = {0, 0, 0};    // the elementary op's own angles
+    double jac[3][3] = {{0}};     // d ang[i] / d gate-field[f]  (theta, phi, lambda)
+};
+
+// Expands one reference gate into elementary ops (the composite sequences of
+// svsim_nvgpu_sin.cuh:1134-1454).  Returns false for an unknown op.
+bool lower_gate(const svb_gate& g, int32_t gate_index, std::vector<EOp>& out);
+
+// Number of elementary ops and of per-gate-model sweeps (half sweeps count 1/2)
+// the reference spends on one op.
+double reference_sweeps(uint32_t op);
+
+// ---------------------------------------------------------------------------------
+// Staged engine: passes and stages.
+//
+// A pass streams the state once through tiles of 2^M amplitudes.  The M "local"
+// qubits of a pass always include the G lowest qubits (so every tile is made of
+// contiguous 2^G-amplitude runs) plus M-G qubits chosen by the planner.  Inside a
+// tile each of the 2^(M-RB) threads holds 2^RB amplitudes in registers; a stage is a
+// run of ops whose dense targets are among the RB register qubits of the stage's
+// layout.  Between stages the tile is re-distributed through shared memory.
+// ---------------------------------------------------------------------------------
+constexpr int RB = 4;            // register bits per thread (16 amplitudes)
+constexpr int MAX_TB = 9;        // thread bits (512 threads)
+constexpr int MAX_M = RB + MAX_TB;
+
+enum LocKind : uint8_t { LOC_REG = 0, LOC_THR = 1, LOC_TILE = 2, LOC_NONE = 3 };
+
+struct DevOp {                   // 80 bytes, read by every thread of a tile
+    uint8_t form;
+    uint8_t tgt;                 // register bit of the dense/CX target
+    uint8_t loc_kind;            // where the diagonal qubit / CX control lives
+    uint8_t loc_bit;             // its register or thread bit
+    uint32_t tile_qubit;         // its global qubit when loc_kind == LOC_TILE
+    double m[8];
+    uint64_t pad;
+};
+static_assert(sizeof(DevOp) == 80, "DevOp layout");
+
+struct DevStage {
+    uint8_t reg_pos[RB];         // local positions held in registers (bit i of k)
+    uint8_t thr_pos[MAX_TB];     // local positions of thread-index bits
+    uint8_t pad[3];
+    int32_t op_begin, op_end;    // range in the DevOp array
+};
+static_assert(sizeof(DevStage) == 24, "DevStage layout");
+
+struct DevPass {
+    uint8_t local_q[MAX_M];      // global qubit of each local position (ascending)
+    uint8_t nonlocal_q[64 - MAX_M];  // global qubits of tile-index bits (ascending)
+    int32_t n_nonlocal;
+    int32_t stage_begin, stage_end;
+    int32_t final_relayout;      // 1: re-distribute to a store layout before writing
+    DevStage store_layout;       // used when final_relayout
+};
+
+struct StagedPlan {
+    int M = 0;                   // tile bits
+    int G = 0;                   // always-local low qubits (swizzle group)
+    std::vector<DevPass> passes;
+    std::vector<DevStage> stages;
+    std::vector<DevOp> ops;
+};
+
+// Builds the staged plan for `ops` on n qubits with tile bits M and low-group G.
+void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& plan);
+
+// ---------------------------------------------------------------------------------
+// Kernel launchers (kernels_apply.cu)
+// ---------------------------------------------------------------------------------
+struct DevPlanBuffers {
+    DevPass* passes = nullptr;
+    DevStage* stages = nullptr;
+    DevOp* ops = nullptr;
+};
+
+// one elementary op, one sweep (per-gate engine)
+template <typename T>
+cudaError_t launch_eop(void* state, int n, const EOp& op, cudaStream_t s);
+// one staged pass
+template <typename T>
+cudaError_t launch_staged_pass(void* state, int n, int M, int pass_index,
+                               const DevPlanBuffers& b, cudaStream_t s);
+template <typename T>
+cudaError_t launch_reset(void* state, int n, cudaStream_t s);
+template <typename T>
+cudaError_t launch_soa_split(const void* state, uint64_t first, uint64_t count,
+                             double* re, double* im, cudaStream_t s);
+template <typename T>
+cudaError_t launch_soa_merge(void* state, uint64_t first, uint64_t count,
+                             const double* re, const double* im, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------
+// Reductions and measurement (measure.cu)
+// ---------------------------------------------------------------------------------
+struct MeasureScratch {
+    double* block_sums = nullptr;   // per block of 2^MEAS_BLOCK_BITS amplitudes
+    double* block_prefix = nullptr; // exclusive prefix of block_sums (+ total at end)
+    double* uniforms = nullptr;
+    uint64_t* samples = nullptr;
+    double* partial = nullptr;      // reduction partials
+    size_t cap_blocks = 0, cap_shots = 0, cap_partial = 0;
+};
+constexpr int MEAS_BLOCK_BITS = 12;
+
+template <typename T>
+cudaError_t measure_device(const void* state, int n, const double* d_uniforms, uint32_t shots,
+                           uint64_t* d_samples, double* d_total, MeasureScratch& scr,
+                           cudaStream_t s);
+size_t measure_scratch_doubles(int n);
+template <typename T>
+cudaError_t expectation_device(const void* state, int n, const svb_pauli_term* d_terms,
+                               int n_terms, double* d_out, double* d_partial, cudaStream_t s);
+constexpr int REDUCE_BLOCKS = 592;   // 4 x 148 SMs
+
+// ---------------------------------------------------------------------------------
+// Adjoint (adjoint.cu)
+// ---------------------------------------------------------------------------------
+// Runs elementary ops on an FP64 device state with the staged engine (per-gate for
+// n < 10); synchronous.
+svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st);
+
+// ---------------------------------------------------------------------------------
+// The handle
+// ---------------------------------------------------------------------------------
+struct Sim {
+    uint32_t n = 0;
+    int device = 0;
+    int precision = SVB_FP64;
+    void* state = nullptr;         // 2^n interleaved complex amplitudes
+    size_t amp_bytes = 16;
+    // circuit and plan
+    std::vector<svb_gate> gates;
+    std::vector<EOp> eops;
+    int engine_req = SVB_ENGINE_AUTO, tile_bits_req = 0, fusion_req = 0;
+    int engine = SVB_ENGINE_PER_GATE;
+    StagedPlan staged;
+    DevPlanBuffers dplan;
+    bool have_circuit = false;
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t capture_stream = nullptr;
+    svb_plan_info info{};
+    // scratch
+    MeasureScratch mscr;
+    double* d_small = nullptr;     // a few doubles for reduction results
+};
+
+void set_error(const std::string& msg);
+
+}  // namespace svb
+
+struct svb_sim : public svb::Sim {};

@@ -1,0 +1,183 @@
+"""ctypes binding of libsvsim_b200.so (C ABI in include/svsim_b200.h).
+
+The library is loaded from the package's lib/ directory.  There is no fallback: if
+the library is missing or was built for another architecture, importing this module
+raises, so nothing silently runs on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .gates import GATE_DTYPE, PARAM_DTYPE, PAULI_DTYPE
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libsvsim_b200.so")
+
+SVB_OK, SVB_ERR_INVALID, SVB_ERR_CUDA, SVB_ERR_OOM, SVB_ERR_UNSUPPORTED, SVB_ERR_STATE = range(6)
+SVB_FP64, SVB_FP32 = 0, 1
+ENGINE_AUTO, ENGINE_PER_GATE, ENGINE_STAGED, ENGINE_FUSED = 0, 1, 2, 3
+
+
+class SvbError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[svb status {status}] {message}")
+        self.status = status
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("n_gates", ctypes.c_uint64), ("n_elementary", ctypes.c_uint64),
+                ("n_passes", ctypes.c_uint64), ("n_sweeps_model", ctypes.c_uint64),
+                ("state_bytes", ctypes.c_double), ("model_bytes", ctypes.c_double),
+                ("moved_bytes", ctypes.c_double), ("plan_bytes", ctypes.c_uint64),
+                ("engine", ctypes.c_int),
+                ("tile_bits", ctypes.c_int)]
+
+
+_lib = None
+
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+_SIGS = {
+    "svb_create": ([ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+    "svb_destroy": ([_vp], ctypes.c_int),
+    "svb_reset_state": ([_vp], ctypes.c_int),
+    "svb_set_circuit": ([_vp, _vp, ctypes.c_size_t], ctypes.c_int),
+    "svb_clear_circuit": ([_vp], ctypes.c_int),
+    "svb_set_engine": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "svb_get_plan_info": ([_vp, ctypes.POINTER(PlanInfo)], ctypes.c_int),
+    "svb_run": ([_vp, _vp], ctypes.c_int),
+    "svb_synchronize": ([_vp], ctypes.c_int),
+    "svb_get_state_soa": ([_vp, _dp, _dp], ctypes.c_int),
+    "svb_set_state_soa": ([_vp, _dp, _dp], ctypes.c_int),
+    "svb_state_device_ptr": ([_vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "svb_measure": ([_vp, _dp, ctypes.c_uint32, _u64p, _dp], ctypes.c_int),
+    "svb_norm2": ([_vp, _dp], ctypes.c_int),
+    "svb_expectation": ([_vp, _vp, ctypes.c_size_t, _dp], ctypes.c_int),
+    "svb_adjoint": ([_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, _vp, ctypes.c_size_t, _dp, _dp],
+                    ctypes.c_int),
+    "svb_last_error": ([], ctypes.c_char_p),
+    "svb_version": ([], ctypes.c_char_p),
+}
+
+
+def lib():
+    """The loaded library; raises if it is absent (no CPU fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libsvsim_b200.so not built ({LIB_PATH}); run "
+                              "`python sv-sim_b200/svsim_b200/build.py`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def check(status: int):
+    if status != SVB_OK:
+        raise SvbError(status, lib().svb_last_error().decode())
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class Handle:
+    """Owns one svb_sim*."""
+
+    def __init__(self, n_qubits: int, device: int = 0, precision: int = SVB_FP64):
+        h = _vp()
+        check(lib().svb_create(n_qubits, device, precision, ctypes.byref(h)))
+        self.ptr = h
+        self.n = n_qubits
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            lib().svb_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- wrappers ------------------------------------------------------------------
+    def set_engine(self, engine=ENGINE_AUTO, tile_bits=0, fusion_width=0):
+        check(lib().svb_set_engine(self.ptr, engine, tile_bits, fusion_width))
+
+    def set_circuit(self, gates: np.ndarray):
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        check(lib().svb_set_circuit(self.ptr, g.ctypes.data, len(g)))
+
+    def clear_circuit(self):
+        check(lib().svb_clear_circuit(self.ptr))
+
+    def reset(self):
+        check(lib().svb_reset_state(self.ptr))
+
+    def run(self, stream: int = 0):
+        check(lib().svb_run(self.ptr, _vp(stream) if stream else None))
+
+    def sync(self):
+        check(lib().svb_synchronize(self.ptr))
+
+    def plan_info(self) -> PlanInfo:
+        info = PlanInfo()
+        check(lib().svb_get_plan_info(self.ptr, ctypes.byref(info)))
+        return info
+
+    def get_state(self):
+        dim = 1 << self.n
+        re = np.empty(dim)
+        im = np.empty(dim)
+        check(lib().svb_get_state_soa(self.ptr, dptr(re), dptr(im)))
+        return re, im
+
+    def set_state(self, re, im):
+        re = np.ascontiguousarray(re, dtype=np.float64)
+        im = np.ascontiguousarray(im, dtype=np.float64)
+        check(lib().svb_set_state_soa(self.ptr, dptr(re), dptr(im)))
+
+    def device_ptr(self):
+        p = _vp()
+        prec = ctypes.c_int()
+        check(lib().svb_state_device_ptr(self.ptr, ctypes.byref(p), ctypes.byref(prec)))
+        return p.value, prec.value
+
+    def measure(self, uniforms):
+        u = np.ascontiguousarray(uniforms, dtype=np.float64)
+        out = np.zeros(len(u), dtype=np.uint64)
+        tot = ctypes.c_double()
+        check(lib().svb_measure(self.ptr, dptr(u), len(u), out.ctypes.data_as(_u64p),
+                                ctypes.byref(tot)))
+        return out, tot.value
+
+    def norm2(self) -> float:
+        v = ctypes.c_double()
+        check(lib().svb_norm2(self.ptr, ctypes.byref(v)))
+        return v.value
+
+    def expectation(self, terms) -> float:
+        t = np.ascontiguousarray(terms, dtype=PAULI_DTYPE)
+        v = ctypes.c_double()
+        check(lib().svb_expectation(self.ptr, t.ctypes.data, len(t), ctypes.byref(v)))
+        return v.value
+
+    def adjoint(self, gates, bindings, n_params, terms):
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        b = np.ascontiguousarray(bindings, dtype=PARAM_DTYPE)
+        t = np.ascontiguousarray(terms, dtype=PAULI_DTYPE)
+        grad = np.zeros(max(n_params, 1))
+        e = ctypes.c_double()
+        check(lib().svb_adjoint(self.ptr, g.ctypes.data, b.ctypes.data, len(g), n_params,
+                                t.ctypes.data, len(t), ctypes.byref(e), dptr(grad)))
+        return e.value, grad[:n_params]

@@ -1,0 +1,176 @@
+// TEST INFRASTRUCTURE: runs a staged plan on the CPU.
+//
+// The planner (sv-sim_b200/csrc/plan.cpp) decides which qubits are local to each pass,
+// how each pass is cut into register layouts and where every op's qubits live.  This
+// file executes such a plan on host memory with the same per-thread helpers the tile
+// kernel uses (staged_core.cuh: swizzle, layout decoding, op application), thread by
+// thread and barrier by barrier, and checks on the way that every shared-memory slot is
+// written exactly once per re-distribution.  Comparing its output with the oracle
+// validates the plan and the kernel's index arithmetic without a GPU.
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "staged_core.cuh"
+
+using namespace svb;
+
+namespace {
+
+template <typename T, int M>
+int run_plan(uint32_t n, const StagedPlan& plan, std::vector<typename VecOf<T>::type>& sv)
+{
+    using V = typename VecOf<T>::type;
+    constexpr int TBITS = M - RB;
+    constexpr int NT = 1 << TBITS;
+    constexpr int NR = 1 << RB;
+    std::vector<V> sm(1u << M);
+    std::vector<int> written(1u << M);
+    std::vector<V> regs((size_t)NT * NR);
+    std::vector<Slots> cur(NT);
+    const uint64_t tiles = 1ull << (n - M);
+
+    auto relayout = [&](const DevStage& to) -> int {
+        std::fill(written.begin(), written.end(), 0);
+        for (int t = 0; t < NT; t++)
+            for (int k = 0; k < NR; k++) {
+                const uint32_t sl = slot_of(cur[t], k);
+                if (sl >= (1u << M) || written[sl]++) return -2;   // not a bijection
+                sm[sl] = regs[(size_t)t * NR + k];
+            }
+        for (int t = 0; t < NT; t++) {
+            Slots nx;
+            make_slots<T, TBITS>(to, t, nx);
+            for (int k = 0; k < NR; k++) regs[(size_t)t * NR + k] = sm[slot_of(nx, k)];
+            cur[t] = nx;
+        }
+        return 0;
+    };
+
+    for (size_t p = 0; p < plan.passes.size(); p++) {
+        const DevPass& P = plan.passes[p];
+        for (uint64_t tile = 0; tile < tiles; tile++) {
+            uint64_t base = 0;
+            for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
+            const DevStage* last = &plan.stages[P.stage_begin];
+            for (int t = 0; t < NT; t++) {
+                GOffs g;
+                make_goffs<TBITS>(*last, P, t, g);
+                for (int k = 0; k < NR; k++) regs[(size_t)t * NR + k] = sv[base | goff_of(g, k)];
+                make_slots<T, TBITS>(*last, t, cur[t]);
+            }
+            for (int s = P.stage_begin; s < P.stage_end; s++) {
+                const DevStage& S = plan.stages[s];
+                if (s != P.stage_begin) {
+                    if (relayout(S)) return -2;
+                    last = &S;
+                }
+                for (int t = 0; t < NT; t++)
+                    for (int o = S.op_begin; o < S.op_end; o++)
+                        apply_devop<T>(&plan.ops[o], &regs[(size_t)t * NR], t, base);
+            }
+            if (P.final_relayout) {
+                if (relayout(P.store_layout)) return -2;
+                last = &P.store_layout;
+            }
+            // stores must cover the tile exactly once as well
+            for (int t = 0; t < NT; t++) {
+                GOffs g;
+                make_goffs<TBITS>(*last, P, t, g);
+                for (int k = 0; k < NR; k++) sv[base | goff_of(g, k)] = regs[(size_t)t * NR + k];
+            }
+        }
+    }
+    return 0;
+}
+
+template <typename T>
+int run_typed(uint32_t n, const StagedPlan& plan, double* re, double* im)
+{
+    using V = typename VecOf<T>::type;
+    const uint64_t dim = 1ull << n;
+    std::vector<V> sv(dim);
+    for (uint64_t i = 0; i < dim; i++) { sv[i].x = (T)re[i]; sv[i].y = (T)im[i]; }
+    int rc;
+    switch (plan.M) {
+    case 10: rc = run_plan<T, 10>(n, plan, sv); break;
+    case 11: rc = run_plan<T, 11>(n, plan, sv); break;
+    case 12: rc = run_plan<T, 12>(n, plan, sv); break;
+    case 13: rc = run_plan<T, 13>(n, plan, sv); break;
+    default: return -1;
+    }
+    for (uint64_t i = 0; i < dim; i++) { re[i] = (double)sv[i].x; im[i] = (double)sv[i].y; }
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Applies `gates` to the SoA state (re, im) in place through the staged plan with tile
+// bits M.  precision: 0 = FP64, 1 = FP32.  Returns 0, -1 for bad arguments, -2 if a
+// re-distribution is not a bijection on the tile.
+int emu_staged_run(uint32_t n, const svb_gate* gates, size_t n_gates, int M, int precision,
+                   double* re, double* im, uint64_t* n_passes, uint64_t* n_stages)
+{
+    if (M < 10 || M > 13 || (int)n < M) return -1;
+    std::vector<EOp> eops;
+    for (size_t i = 0; i < n_gates; i++)
+        if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
+    StagedPlan plan;
+    plan_staged(eops, (int)n, M, precision == 0 ? 3 : 4, plan);
+    if (n_passes) *n_passes = plan.passes.size();
+    if (n_stages) *n_stages = plan.stages.size();
+    return precision == 0 ? run_typed<double>(n, plan, re, im) : run_typed<float>(n, plan, re, im);
+}
+
+// Pass / stage / relayout counts of the plan without executing it.
+int emu_plan_stats(uint32_t n, const svb_gate* gates, size_t n_gates, int M, int precision,
+                   uint64_t* n_passes, uint64_t* n_stages, uint64_t* n_final_relayouts,
+                   uint64_t* n_elementary)
+{
+    std::vector<EOp> eops;
+    for (size_t i = 0; i < n_gates; i++)
+        if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
+    StagedPlan plan;
+    plan_staged(eops, (int)n, M, precision == 0 ? 3 : 4, plan);
+    *n_passes = plan.passes.size();
+    *n_stages = plan.stages.size();
+    uint64_t f = 0;
+    for (const DevPass& P : plan.passes) f += P.final_relayout;
+    *n_final_relayouts = f;
+    *n_elementary = eops.size();
+    return 0;
+}
+
+}  // extern "C"
+
+extern "C" int emu_plan_dump(uint32_t n, const svb_gate* gates, size_t n_gates, int M, int precision)
+{
+    std::vector<EOp> eops;
+    for (size_t i = 0; i < n_gates; i++)
+        if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
+    StagedPlan plan;
+    plan_staged(eops, (int)n, M, precision == 0 ? 3 : 4, plan);
+    const int TB = M - RB;
+    for (size_t p = 0; p < plan.passes.size(); p++) {
+        const DevPass& P = plan.passes[p];
+        printf("pass %zu local:", p);
+        for (int j = 0; j < M; j++) printf(" %d", P.local_q[j]);
+        printf(" final_relayout=%d\n", P.final_relayout);
+        for (int s = P.stage_begin; s < P.stage_end; s++) {
+            const DevStage& S = plan.stages[s];
+            printf("  stage %d regs(pos):", s);
+            for (int i = 0; i < RB; i++) printf(" %d", S.reg_pos[i]);
+            printf(" thr(pos):");
+            for (int b = 0; b < TB; b++) printf(" %d", S.thr_pos[b]);
+            printf("\n");
+            for (int o = S.op_begin; o < S.op_end; o++) {
+                const DevOp& d = plan.ops[o];
+                printf("    form=%d tgt=%d loc=%d bit=%d tq=%u\n", d.form, d.tgt, d.loc_kind, d.loc_bit, d.tile_qubit);
+            }
+        }
+    }
+    fflush(stdout);
+    return 0;
+}

@@ -1,0 +1,104 @@
+"""Host logic of the staged engine: plans executed on the CPU by tests/native's emulator
+(the tile kernel's own index helpers) must reproduce the oracle."""
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from conftest import fidelity
+from svsim_b200 import circuits, gates as G
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+@pytest.fixture(scope="module")
+def emu():
+    import build_emulator
+    lib = ctypes.CDLL(build_emulator.build())
+    return lib
+
+
+def run_emu(lib, n, gates, M, precision=0, state=None):
+    if state is None:
+        re = np.zeros(1 << n)
+        im = np.zeros(1 << n)
+        re[0] = 1.0
+    else:
+        re, im = state[0].copy(), state[1].copy()
+    np_, ns = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib.emu_staged_run(n, gates.ctypes.data, ctypes.c_size_t(len(gates)), M, precision,
+                            re.ctypes.data_as(_dp), im.ctypes.data_as(_dp), ctypes.byref(np_),
+                            ctypes.byref(ns))
+    assert rc == 0, f"emulator rc {rc}"
+    return re, im, np_.value
+
+
+def mixed_circuit(n, reps, seed):
+    rng = np.random.default_rng(seed)
+    gl = G.from_array(circuits.random_matching_circuit(n, 1, seed=seed))
+    for _ in range(reps):
+        for name in G.OP_NAMES:
+            qs = [int(x) for x in rng.permutation(n)[:G.N_QUBITS[name]]]
+            npar = {"U3": 3, "U2": 2, "CU3": 3}.get(name, 1 if name in (
+                "U1", "RX", "RY", "RZ", "CRX", "CRY", "CRZ", "CU1", "RXX", "RZZ", "RYY", "R") else 0)
+            gl.append(G.FACTORIES[name](*([rng.uniform(-math.pi, math.pi) for _ in range(npar)] + qs)))
+    return G.to_array(gl)
+
+
+@pytest.mark.parametrize("n,M", [(10, 10), (12, 10), (12, 11), (12, 12), (13, 12), (15, 12)])
+def test_staged_plan_random_matching_fp64(emu, oracle, n, M):
+    g = circuits.random_matching_circuit(n, 10, seed=n * 31 + M)
+    re, im, passes = run_emu(emu, n, g, M)
+    ore, oim = oracle.run(n, g)
+    assert np.max(np.abs(re - ore)) < 1e-13 and np.max(np.abs(im - oim)) < 1e-13
+    assert passes < len(g)
+
+
+@pytest.mark.parametrize("M", [10, 11, 12])
+def test_staged_plan_every_op_fp64(emu, oracle, M):
+    """All 38 ops, including the non-unitary SRN and R, interleaved at random."""
+    n = 12
+    g = mixed_circuit(n, 4, seed=M)
+    re, im, _ = run_emu(emu, n, g, M)
+    ore, oim = oracle.run(n, g)
+    assert np.max(np.abs(re - ore)) < 1e-12 and np.max(np.abs(im - oim)) < 1e-12
+
+
+@pytest.mark.parametrize("M", [11, 12, 13])
+def test_staged_plan_every_op_fp32(emu, oracle, M):
+    n = 13
+    g = mixed_circuit(n, 3, seed=100 + M)
+    re, im, _ = run_emu(emu, n, g, M, precision=1)
+    ore, oim = oracle.run(n, g)
+    assert 1 - fidelity(re + 1j * im, ore + 1j * oim) < 1e-6
+
+
+def test_staged_plan_from_arbitrary_state(emu, oracle):
+    n = 11
+    rng = np.random.default_rng(5)
+    st = (rng.standard_normal(1 << n), rng.standard_normal(1 << n))
+    g = mixed_circuit(n, 2, seed=9)
+    re, im, _ = run_emu(emu, n, g, 11, state=st)
+    ore, oim = oracle.run(n, g, state=st)
+    assert np.max(np.abs(re - ore)) < 1e-11 and np.max(np.abs(im - oim)) < 1e-11
+
+
+def test_srn_is_ordered_against_complex_gates(emu, oracle):
+    """SRN (svsim_nvgpu_sin.cuh:894-907) is only real-linear: moving it past a complex
+    gate on another qubit changes the result, so the plan must not reorder it."""
+    g = G.to_array([G.H(2), G.SRN(0), G.W(5), G.U2(-0.68, 0.36, 2)])
+    re, im, _ = run_emu(emu, 12, g, 12)
+    ore, oim = oracle.run(12, g)
+    assert np.max(np.abs(re - ore)) < 1e-14 and np.max(np.abs(im - oim)) < 1e-14
+
+
+def test_plan_pass_counts_headline_circuit(emu):
+    """The n=30 depth-40 circuit (1,800 gates) needs far fewer passes than sweeps."""
+    g = circuits.random_matching_circuit(30, 40)
+    a, b, c, d = (ctypes.c_uint64() for _ in range(4))
+    rc = emu.emu_plan_stats(30, g.ctypes.data, ctypes.c_size_t(len(g)), 12, 0, ctypes.byref(a),
+                            ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
+    assert rc == 0
+    assert d.value == 1800
+    assert a.value <= 80          # passes (each one read + one write of the state)
