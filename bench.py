@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary forms")
+    ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--qubits", type=int, default=N_QUBITS,
+                    help="state size (smaller cases are for profiling only)")
+    ap.add_argument("--tile-bits", type=int, default=12)
     return ap.parse_args()
 
 
@@ -198,11 +202,12 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     device = local
     torch.cuda.set_device(device)
-    circuit = circuits.random_matching_circuit(N_QUBITS, DEPTH, seed=SEED)
+    nq = args.qubits
+    circuit = circuits.random_matching_circuit(nq, DEPTH, seed=SEED)
     n_gates = len(circuit)
 
-    h = nat.Handle(N_QUBITS, device, nat.SVB_FP64)
-    h.set_engine(nat.ENGINE_STAGED, 12, 0)
+    h = nat.Handle(nq, device, nat.SVB_FP64)
+    h.set_engine(nat.ENGINE_STAGED, args.tile_bits, 0)
     h.set_circuit(circuit)
     info = h.plan_info()
     stream = torch.cuda.current_stream(device)
@@ -278,7 +283,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_qubits": N_QUBITS, "depth": DEPTH, "gates": n_gates,
+        "config": {"workload": WORKLOAD, "n_qubits": nq, "depth": DEPTH, "gates": n_gates,
                    "seed": SEED, "engine": "staged", "tile_bits": int(info.tile_bits),
                    "passes": passes, "parallelism": f"replicas x{world}",
                    "l2": "16 GiB state > 126 MB L2: every step streams from HBM, no flush"},
@@ -290,13 +295,15 @@ def run_ours(args):
     del h
     torch.cuda.empty_cache()
 
-    if rank == 0 and world == 1:
+    if nq != N_QUBITS:
+        out["config"]["workload"] = f"profiling case: n={nq} (not the headline workload)"
+    if rank == 0 and world == 1 and not args.no_baseline and nq == N_QUBITS:
         threads = os.cpu_count() or 1
         try:
             out["cpu_baseline"] = cpu_reference_rate(circuit, threads)
         except Exception as e:  # the baseline is reported, never required
             out["cpu_baseline"] = {"value": None, "error": str(e)}
-    if rank == 0 and not args.no_extras and world == 1:
+    if rank == 0 and not args.no_extras and world == 1 and nq == N_QUBITS:
         out["forms"] = secondary_forms(device, circuit)
     if world > 1:
         torch.distributed.barrier()

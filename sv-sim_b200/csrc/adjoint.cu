@@ -81,7 +81,7 @@ k_adj_step(double2* __restrict__ psi, double2* __restrict__ lam, uint64_t half, 
     }
     for (int d = 0; d < nd; d++) {
         const double s = block_sum(acc[d], red);
-        if (threadIdx.x == 0) partial[(size_t)d * gridDim.x + blockIdx.x] = s;
+        if (threadIdx.x == 0) partial[(size_t)d * ADJ_BLOCKS + blockIdx.x] = s;
     }
 }
 
@@ -146,7 +146,8 @@ k_inner_re(const double2* __restrict__ a, const double2* __restrict__ b, uint64_
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
-// results[r] = sum of partial[r * nblocks .. +nblocks), one warp per result
+// results[r] = sum of partial[r * ADJ_BLOCKS + i], i < nblocks (the blocks the producing
+// kernels ran with); one warp per result, fixed order
 __global__ void k_reduce_rows(const double* __restrict__ partial, int nblocks, int rows,
                               double* __restrict__ results)
 {
@@ -154,7 +155,7 @@ __global__ void k_reduce_rows(const double* __restrict__ partial, int nblocks, i
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (row >= rows) return;
     double s = 0.0;
-    for (int i = lane; i < nblocks; i += 32) s += partial[(size_t)row * nblocks + i];
+    for (int i = lane; i < nblocks; i += 32) s += partial[(size_t)row * ADJ_BLOCKS + i];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) results[row] = s;
@@ -247,7 +248,7 @@ bool inverse_op(const EOp& e, EOp& inv)
     case F_Y:  c1(0, 0, 0, -1, 0, 1, 0, 0); return true;
     case F_H:  c1(S2I, 0, S2I, 0, S2I, 0, -S2I, 0); return true;
     case F_W:  c1(S2I, 0, 0, S2I, 0, S2I, S2I, 0); return true;
-    case F_RX: c1(e.m[0], 0, 0, e.m[1], 0, e.m[1], e.m[0], 0); return true;   // RX(-theta)
+    case F_RX: c1(e.m[0], 0, 0, -e.m[1], 0, -e.m[1], e.m[0], 0); return true;  // RX(-theta)
     case F_RY: c1(e.m[0], 0, e.m[2], 0, e.m[1], 0, e.m[3], 0); return true;   // transpose
     case F_Z:  dg(1, 0, -1, 0); return true;
     case F_S:  dg(1, 0, 0, -1); return true;
@@ -427,7 +428,7 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
         }
     }
     if (!slots.empty())
-        k_reduce_rows<<<(unsigned)((slots.size() * 32 + 255) / 256), 256>>>(partial, ADJ_BLOCKS,
+        k_reduce_rows<<<(unsigned)((slots.size() * 32 + 255) / 256), 256>>>(partial, (int)gp,
                                                                           (int)slots.size(), results);
     std::vector<double> host(slots.size() + 1);
     if ((err = cudaMemcpy(host.data(), results, host.size() * sizeof(double), cudaMemcpyDeviceToHost)) !=

@@ -95,7 +95,9 @@ struct PassBuilder {
         for (int i = 0; i < RB; i++) st.reg_pos[i] = (uint8_t)regs[i];
     }
 
-    void build(uint64_t L, const std::vector<int>& taken) {
+    // Builds one pass from `taken` (program order).  Returns the ops that did not fit
+    // in MAX_PASS_STAGES stages; they are left for later passes.
+    std::vector<int> build(uint64_t L, const std::vector<int>& taken) {
         DevPass P;
         std::memset(&P, 0, sizeof(P));
         int pos_of[64];
@@ -111,7 +113,10 @@ struct PassBuilder {
         std::vector<int> remaining = taken, rest, stage_ops;
         bool first = true;
         DevStage last{};
+        int n_stages = 0;
         do {
+            if (n_stages == MAX_PASS_STAGES) break;
+            n_stages++;
             // register positions: first distinct target positions in program order
             std::vector<int> regs;
             for (int i : remaining) {
@@ -164,6 +169,7 @@ struct PassBuilder {
             fill_threads(regs, P.store_layout, true);
         }
         plan.passes.push_back(P);
+        return remaining;
     }
 
     void locate(uint32_t q, const std::vector<int>& regs, const DevStage& st, const int* pos_of,
@@ -245,10 +251,11 @@ void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& p
             }
             taken.push_back((int)i);
             done[i] = 1;
+            if ((int)taken.size() == MAX_PASS_OPS) break;
         }
         for (int q = 0; nL < M && q < n; q++)
             if (!((L >> q) & 1)) { L |= bit(q); nL++; }
-        pb.build(L, taken);
+        for (int i : pb.build(L, taken)) done[i] = 0;
     }
 }
 

@@ -74,18 +74,20 @@ double reference_sweeps(uint32_t op);
 // layout.  Between stages the tile is re-distributed through shared memory.
 // ---------------------------------------------------------------------------------
 constexpr int RB = 4;            // register bits per thread (16 amplitudes)
+constexpr int MAX_PASS_OPS = 256;     // ops of one pass, staged in shared memory
+constexpr int MAX_PASS_STAGES = 64;   // stages of one pass
 constexpr int MAX_TB = 9;        // thread bits (512 threads)
 constexpr int MAX_M = RB + MAX_TB;
 
 enum LocKind : uint8_t { LOC_REG = 0, LOC_THR = 1, LOC_TILE = 2, LOC_NONE = 3 };
 
 struct DevOp {                   // 80 bytes, read by every thread of a tile
+    double m[8];                 // coefficients first: 16-byte aligned for vector loads
     uint8_t form;
     uint8_t tgt;                 // register bit of the dense/CX target
     uint8_t loc_kind;            // where the diagonal qubit / CX control lives
     uint8_t loc_bit;             // its register or thread bit
     uint32_t tile_qubit;         // its global qubit when loc_kind == LOC_TILE
-    double m[8];
     uint64_t pad;
 };
 static_assert(sizeof(DevOp) == 80, "DevOp layout");
