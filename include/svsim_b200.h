@@ -163,6 +163,11 @@ svb_status svb_norm2(svb_sim* sim, double* out);
 svb_status svb_expectation(svb_sim* sim, const svb_pauli_term* terms, size_t n_terms,
                            double* out);
 
+/* Compares the states of two handles of equal size and device, either precision:
+ * fidelity = |<a|b>|^2 / (<a|a><b|b>) and max_i |a_i - b_i|, both in FP64 (the
+ * accuracy report of the FP32 engines against FP64; no reference counterpart). */
+svb_status svb_compare_states(svb_sim* a, svb_sim* b, double* fidelity, double* max_abs_diff);
+
 /* ---- differentiation (no reference counterpart) --------------------------------- */
 
 /* Adjoint differentiation of E(p) = <psi(p)| H |psi(p)>, psi(p) = U(p)|0..0>:

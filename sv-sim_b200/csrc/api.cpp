@@ -65,6 +65,12 @@ void free_plan(Sim* s)
     cudaFree(s->dplan.ops);
     s->dplan = DevPlanBuffers{};
     s->staged = StagedPlan{};
+    cudaFree(s->dfused.passes);
+    cudaFree(s->dfused.blocks);
+    cudaFree(s->dfused.gates);
+    cudaFree(s->dfused.err);
+    s->dfused = DevFusedBuffers{};
+    s->fused = FusedPlan{};
     s->eops.clear();
     s->gates.clear();
     s->have_circuit = false;
@@ -134,6 +140,15 @@ bool staged_supported(int precision, int M)
 svb_status launch_all(Sim* s, cudaStream_t st)
 {
     const int n = (int)s->n;
+    if (s->engine == SVB_ENGINE_FUSED) {
+        const FusedPlan& F = s->fused;
+        for (size_t p = 0; p < F.passes.size(); p++) {
+            cudaError_t e = launch_fused_pass(s->state, n, F.k, (int)p, F.passes[p].n_blocks, 0,
+                                              s->dfused, st);
+            if (e != cudaSuccess) return cuda_fail(e, "fused pass launch");
+        }
+        return SVB_OK;
+    }
     if (s->engine == SVB_ENGINE_STAGED) {
         for (size_t p = 0; p < s->staged.passes.size(); p++) {
             cudaError_t e = dispatch_prec(s->precision, [&](auto t) {
@@ -281,8 +296,8 @@ svb_status svb_set_engine(svb_sim* s, int engine, int tile_bits, int fusion_widt
         return invalid("svb_set_engine: the fused engine runs FP32 states");
     if (tile_bits != 0 && !staged_supported(s->precision, tile_bits))
         return invalid("svb_set_engine: tile_bits must be 10..12 (FP64) or 11..13 (FP32)");
-    if (fusion_width != 0 && (fusion_width < 2 || fusion_width > 6))
-        return invalid("svb_set_engine: fusion_width must be 2..6");
+    if (fusion_width != 0 && (fusion_width < FT_MIN_K || fusion_width > FT_MAX_K))
+        return invalid("svb_set_engine: fusion_width must be 3..5");
     s->engine_req = engine;
     s->tile_bits_req = tile_bits;
     s->fusion_req = fusion_width;
@@ -327,8 +342,14 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
     if (engine == SVB_ENGINE_AUTO)
         engine = (staged_supported(s->precision, M) && n >= M) ? SVB_ENGINE_STAGED : SVB_ENGINE_PER_GATE;
     if (engine == SVB_ENGINE_FUSED) {
-        set_error("svb_set_circuit: the fused engine is not available in this build");
-        return SVB_ERR_UNSUPPORTED;
+        if (s->precision != SVB_FP32 || n < FT_TILE_BITS) {
+            set_error("svb_set_circuit: the fused engine needs an FP32 state of >= 12 qubits");
+            return SVB_ERR_UNSUPPORTED;
+        }
+        if (!fusable(s->eops)) {
+            set_error("svb_set_circuit: SRN is not complex-linear and cannot be fused");
+            return SVB_ERR_UNSUPPORTED;
+        }
     }
     if (engine == SVB_ENGINE_STAGED && !(staged_supported(s->precision, M) && n >= M)) {
         set_error("svb_set_circuit: the staged engine needs n_qubits >= tile bits (10 FP64, 11 FP32)");
@@ -343,7 +364,33 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
     s->info.state_bytes = sb;
     s->info.model_bytes = 2.0 * sb * sweeps;
     s->info.engine = engine;
-    if (engine == SVB_ENGINE_STAGED) {
+    if (engine == SVB_ENGINE_FUSED) {
+        const int k = s->fusion_req ? s->fusion_req : FT_MAX_K;
+        plan_fused(s->eops, n, k, s->fused);
+        const FusedPlan& F = s->fused;
+        SVB_CUDA(cudaMalloc(&s->dfused.passes, std::max<size_t>(1, F.passes.size()) * sizeof(FusedPass)),
+                 "cudaMalloc(plan)");
+        SVB_CUDA(cudaMalloc(&s->dfused.blocks, std::max<size_t>(1, F.blocks.size()) * sizeof(FusedBlock)),
+                 "cudaMalloc(plan)");
+        SVB_CUDA(cudaMalloc(&s->dfused.gates, std::max<size_t>(4, F.gates.size()) * sizeof(float)),
+                 "cudaMalloc(plan)");
+        SVB_CUDA(cudaMalloc(&s->dfused.err, sizeof(int)), "cudaMalloc(flag)");
+        SVB_CUDA(cudaMemset(s->dfused.err, 0, sizeof(int)), "cudaMemset");
+        if (!F.passes.empty())
+            SVB_CUDA(cudaMemcpy(s->dfused.passes, F.passes.data(), F.passes.size() * sizeof(FusedPass),
+                                cudaMemcpyHostToDevice), "plan upload");
+        if (!F.blocks.empty())
+            SVB_CUDA(cudaMemcpy(s->dfused.blocks, F.blocks.data(), F.blocks.size() * sizeof(FusedBlock),
+                                cudaMemcpyHostToDevice), "plan upload");
+        if (!F.gates.empty())
+            SVB_CUDA(cudaMemcpy(s->dfused.gates, F.gates.data(), F.gates.size() * sizeof(float),
+                                cudaMemcpyHostToDevice), "plan upload");
+        s->info.n_passes = F.passes.size();
+        s->info.tile_bits = FT_TILE_BITS;
+        s->info.plan_bytes = F.passes.size() * sizeof(FusedPass) + F.blocks.size() * sizeof(FusedBlock) +
+                             F.gates.size() * sizeof(float);
+        s->info.moved_bytes = 2.0 * sb * (double)F.passes.size();
+    } else if (engine == SVB_ENGINE_STAGED) {
         const int G = s->precision == SVB_FP64 ? 3 : 4;
         plan_staged(s->eops, n, M, G, s->staged);
         const StagedPlan& P = s->staged;
@@ -431,6 +478,15 @@ svb_status svb_synchronize(svb_sim* s)
     if (!s) return invalid("svb_synchronize: NULL handle");
     SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
     SVB_CUDA(cudaDeviceSynchronize(), "kernel execution");
+    if (s->engine == SVB_ENGINE_FUSED && s->dfused.err) {
+        int flag = 0;
+        SVB_CUDA(cudaMemcpy(&flag, s->dfused.err, sizeof(int), cudaMemcpyDeviceToHost), "flag read");
+        if (flag) {
+            cudaMemset(s->dfused.err, 0, sizeof(int));
+            set_error("fused kernel: a tensor-core completion wait timed out");
+            return SVB_ERR_CUDA;
+        }
+    }
     return SVB_OK;
 }
 
@@ -524,6 +580,33 @@ svb_status svb_norm2(svb_sim* s, double* out)
 {
     if (!out) return invalid("svb_norm2: NULL output");
     return svb_measure(s, nullptr, 0, nullptr, out);
+}
+
+svb_status svb_compare_states(svb_sim* a, svb_sim* b, double* fidelity, double* max_abs_diff)
+{
+    if (!a || !b) return invalid("svb_compare_states: NULL handle");
+    if (a->n != b->n || a->device != b->device)
+        return invalid("svb_compare_states: states differ in size or device");
+    SVB_CUDA(cudaSetDevice(a->device), "cudaSetDevice");
+    double* buf = nullptr;
+    SVB_CUDA(cudaMalloc(&buf, (5 + 5 * REDUCE_BLOCKS) * sizeof(double)), "cudaMalloc(compare)");
+    cudaError_t e;
+    const int n = (int)a->n;
+    if (a->precision == SVB_FP64 && b->precision == SVB_FP64)
+        e = compare_device<double, double>(a->state, b->state, n, buf, buf + 5, nullptr);
+    else if (a->precision == SVB_FP64)
+        e = compare_device<double, float>(a->state, b->state, n, buf, buf + 5, nullptr);
+    else if (b->precision == SVB_FP64)
+        e = compare_device<float, double>(a->state, b->state, n, buf, buf + 5, nullptr);
+    else
+        e = compare_device<float, float>(a->state, b->state, n, buf, buf + 5, nullptr);
+    double v[5] = {0, 0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(v, buf, sizeof(v), cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    if (e != cudaSuccess) return cuda_fail(e, "svb_compare_states");
+    if (fidelity) *fidelity = (v[2] > 0 && v[3] > 0) ? (v[0] * v[0] + v[1] * v[1]) / (v[2] * v[3]) : 0.0;
+    if (max_abs_diff) *max_abs_diff = v[4];
+    return SVB_OK;
 }
 
 svb_status svb_expectation(svb_sim* s, const svb_pauli_term* terms, size_t n_terms, double* out)

@@ -1,0 +1,320 @@
+// Fused tensor-core engine: tcgen05 MMAs on an FP32 state tile in shared memory.
+//
+// One persistent CTA per SM (4 warps = the 128 TMEM lanes) walks the tiles of a pass.
+// For a tile of 4096 amplitudes (12 local qubits) and a fused block on k target qubits,
+// the tile is viewed as X[n][kk]: rows n = the 2^(12-k) values of the other local
+// qubits, kk = 2a + re/im for the 2^k target values a.  The block's real-form gate
+// G[m'][kk] (2^(k+1) square) is applied as
+//        D[n][m'] = sum_kk X[n][kk] G[m'][kk]
+// with tcgen05.mma.kind::tf32 (M = 128 rows per MMA, N = 2^(k+1), K = 8 per
+// instruction) accumulating in TMEM, in three products X_hi G_hi + X_hi G_lo + X_lo G_hi
+// (split TF32: hi = x rounded to TF32, lo = x - hi), so the result keeps ~FP32
+// accuracy.  Both operands sit in shared memory in the canonical K-major, no-swizzle
+// layout (8-row x 16-byte core matrices).  Each thread then reads its D row (one row n,
+// all 2^k amplitudes) with tcgen05.ld and scatters it, split again into hi/lo, into the
+// operand layout of the next block — or, after the last block, into a plain staging
+// copy of the tile that is written back to HBM.
+//
+// Every wait on the MMA-completion mbarrier is bounded; on timeout the kernel records
+// an error, releases its tensor memory and returns.
+#include <cstdint>
+
+#include "svb_internal.h"
+
+namespace svb {
+namespace {
+
+constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kWaitLimit = 1u << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// canonical K-major, no-swizzle shared-memory descriptor
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;                 // descriptor version (sm_100)
+    return d;                               // base offset 0, LBO mode 0, no swizzle
+}
+
+// kind::tf32 instruction descriptor: D f32, A/B tf32, both K-major, M = 128
+__host__ __device__ constexpr uint32_t umma_idesc_tf32(uint32_t n)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                         uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate),
+          "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t it = 0; it < kWaitLimit; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ float tf32_rna(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// 16 consecutive TMEM columns of this warp's 32 lanes
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+struct FusedSmem {
+    static constexpr uint32_t x_bytes = 4096u * 2u * 4u;                  // one plane: 32 KiB
+    static constexpr uint32_t gate_bytes_max = 2u * 64u * 64u * 4u;       // hi+lo for k = 5
+    static constexpr uint32_t x_hi = 0;
+    static constexpr uint32_t x_lo = x_hi + x_bytes;
+    static constexpr uint32_t gates = x_lo + x_bytes;
+    static constexpr uint32_t blocks = gates + FT_MAX_BLOCKS * gate_bytes_max;
+    static constexpr uint32_t pass = blocks + FT_MAX_BLOCKS * sizeof(FusedBlock);
+    static constexpr uint32_t misc = pass + sizeof(FusedPass);
+    static constexpr uint32_t total = misc + 64;
+    static_assert(gates % 16 == 0 && blocks % 16 == 0 && pass % 16 == 0 && misc % 16 == 0, "align");
+};
+
+// Writes amplitude (re, im) of local index l into the state operand of block B.
+__device__ __forceinline__ void put_operand(float* xh, float* xl, const FusedBlock& B, uint32_t l,
+                                            float re, float im)
+{
+    const uint32_t w = B.off_lo[l & 63u] + B.off_hi[l >> 6];
+    const float hr = tf32_rna(re), hi = tf32_rna(im);
+    xh[w] = hr;
+    xh[w + 1] = hi;
+    xl[w] = re - hr;
+    xl[w + 1] = im - hi;
+}
+
+template <int K>
+__global__ void __launch_bounds__(FT_THREADS, 1)
+k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
+        const FusedBlock* __restrict__ blocks, const float* __restrict__ gates, int pass_index,
+        uint64_t tiles, int* __restrict__ err)
+{
+    constexpr int N = 1 << (K + 1);                 // real gate dimension = MMA N = K extent
+    constexpr int ROWS = 1 << (FT_TILE_BITS - K);   // rows of the state operand
+    constexpr int MBLK = ROWS / 128;                // M = 128 blocks
+    constexpr int KSTEPS = N / 8;                   // tf32 MMA K = 8
+    constexpr uint32_t GATE_WORDS = 2u * N * N;     // hi + lo planes
+    constexpr uint32_t IDESC = umma_idesc_tf32(N);
+    static_assert(MBLK * N <= (int)kTmemCols, "TMEM columns");
+
+    extern __shared__ __align__(128) unsigned char sm[];
+    float* xh = reinterpret_cast<float*>(sm + FusedSmem::x_hi);
+    float* xl = reinterpret_cast<float*>(sm + FusedSmem::x_lo);
+    float* sg = reinterpret_cast<float*>(sm + FusedSmem::gates);
+    FusedBlock* sb = reinterpret_cast<FusedBlock*>(sm + FusedSmem::blocks);
+    FusedPass* sp = reinterpret_cast<FusedPass*>(sm + FusedSmem::pass);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + FusedSmem::misc);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + FusedSmem::misc + 16);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+
+    // -- stage the pass, its blocks and their gate operands in shared memory
+    {
+        const FusedPass& gp = passes[pass_index];
+        const uint4* src = reinterpret_cast<const uint4*>(&gp);
+        uint4* dst = reinterpret_cast<uint4*>(sp);
+        for (int w = tid; w < (int)(sizeof(FusedPass) / 16); w += FT_THREADS) dst[w] = src[w];
+    }
+    __syncthreads();
+    const int nb = sp->n_blocks;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(blocks + sp->block_begin);
+        uint4* dst = reinterpret_cast<uint4*>(sb);
+        for (int w = tid; w < nb * (int)(sizeof(FusedBlock) / 16); w += FT_THREADS) dst[w] = src[w];
+    }
+    __syncthreads();
+    for (int b = 0; b < nb; b++) {
+        const uint4* src = reinterpret_cast<const uint4*>(gates + sb[b].gate_word);
+        uint4* dst = reinterpret_cast<uint4*>(sg + b * GATE_WORDS);
+        for (int w = tid; w < (int)(GATE_WORDS / 4); w += FT_THREADS) dst[w] = src[w];
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_slot)), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t x_hi_a = smem_u32(xh), x_lo_a = smem_u32(xl), g_a = smem_u32(sg);
+    const FusedPass& P = *sp;
+    uint32_t parity = 0;
+    bool ok = true;
+
+    for (uint64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        uint64_t base = 0;
+        for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
+        // load the tile (thread t owns local indices t + 128 j) into block 0's operand
+#pragma unroll 4
+        for (int j = 0; j < 32; j++) {
+            const uint32_t l = (uint32_t)tid + 128u * (uint32_t)j;
+            const float2 a = sv[base + P.g_lo[l & 63u] + P.g_hi[l >> 6]];
+            put_operand(xh, xl, sb[0], l, a.x, a.y);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+
+        for (int b = 0; b < nb && ok; b++) {
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t gh = g_a + (uint32_t)b * GATE_WORDS * 4u;
+                const uint32_t gl = gh + (uint32_t)N * N * 4u;
+#pragma unroll
+                for (int mb = 0; mb < MBLK; mb++) {
+                    const uint32_t d = tmem + (uint32_t)(mb * N);
+                    const uint32_t aoff = (uint32_t)mb * 16u * 128u;
+#pragma unroll
+                    for (int s = 0; s < KSTEPS; s++) {
+                        const uint32_t ka = (uint32_t)s * 2u * (ROWS * 16u);
+                        const uint32_t kb = (uint32_t)s * 2u * (N * 16u);
+                        const uint64_t dah = umma_desc(x_hi_a + aoff + ka, ROWS * 16u, 128u);
+                        const uint64_t dal = umma_desc(x_lo_a + aoff + ka, ROWS * 16u, 128u);
+                        const uint64_t dbh = umma_desc(gh + kb, N * 16u, 128u);
+                        const uint64_t dbl = umma_desc(gl + kb, N * 16u, 128u);
+                        mma_tf32(d, dah, dbh, IDESC, s > 0 ? 1u : 0u);
+                        mma_tf32(d, dah, dbl, IDESC, 1u);
+                        mma_tf32(d, dal, dbh, IDESC, 1u);
+                    }
+                }
+                mma_commit(bar);
+            }
+            const bool got = mbar_wait(bar, parity);
+            parity ^= 1u;
+            ok = __syncthreads_and(got ? 1 : 0) != 0;
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // this thread's D rows: n = 32 warp + lane + 128 mb
+            const FusedBlock& B = sb[b];
+            const bool last = (b == nb - 1);
+            float2* stage = reinterpret_cast<float2*>(xh);     // plain tile copy after the last block
+            float dv[MBLK][N];
+#pragma unroll
+            for (int mb = 0; mb < MBLK; mb++)
+#pragma unroll
+                for (int c = 0; c < N; c += 16)
+                    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mb * N + c), &dv[mb][c]);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();   // every row is read before the operand planes are overwritten
+#pragma unroll
+            for (int mb = 0; mb < MBLK; mb++) {
+                const uint32_t n = (uint32_t)(warp * 32 + (tid & 31) + 128 * mb);
+                const uint32_t nl = B.n_lo[n & 31u] | B.n_hi[n >> 5];
+#pragma unroll
+                for (int a = 0; a < (1 << K); a++) {
+                    const uint32_t l = nl | B.a_sc[a];
+                    const float re = dv[mb][2 * a], im = dv[mb][2 * a + 1];
+                    if (last) stage[l] = make_float2(re, im);
+                    else put_operand(xh, xl, sb[b + 1], l, re, im);
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+        }
+        if (!ok) break;
+        // store the tile
+        const float2* stage = reinterpret_cast<const float2*>(xh);
+#pragma unroll 4
+        for (int j = 0; j < 32; j++) {
+            const uint32_t l = (uint32_t)tid + 128u * (uint32_t)j;
+            sv[base + P.g_lo[l & 63u] + P.g_hi[l >> 6]] = stage[l];
+        }
+        __syncthreads();
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+template <int K>
+cudaError_t launch_k(void* state, int n, int pass_index, const DevFusedBuffers& b, cudaStream_t s)
+{
+    static int sms[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && sms[dev] == 0) {
+        cudaError_t e = cudaFuncSetAttribute(k_fused<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)FusedSmem::total);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+    }
+    const uint64_t tiles = 1ull << (n - FT_TILE_BITS);
+    const uint64_t grid = tiles < (uint64_t)sms[dev] ? tiles : (uint64_t)sms[dev];
+    k_fused<K><<<(unsigned)grid, FT_THREADS, FusedSmem::total, s>>>(
+        static_cast<float2*>(state), b.passes, b.blocks, b.gates, pass_index, tiles, b.err);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_fused_pass(void* state, int n, int k, int pass_index, int n_blocks,
+                              int gate_words_per_block, const DevFusedBuffers& b, cudaStream_t s)
+{
+    (void)n_blocks;
+    (void)gate_words_per_block;
+    if (n < FT_TILE_BITS) return cudaErrorInvalidValue;
+    switch (k) {
+    case 3: return launch_k<3>(state, n, pass_index, b, s);
+    case 4: return launch_k<4>(state, n, pass_index, b, s);
+    case 5: return launch_k<5>(state, n, pass_index, b, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace svb

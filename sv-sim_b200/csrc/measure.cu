@@ -202,7 +202,73 @@ __global__ void k_sum_partials(const double* __restrict__ partial, int count, do
     if (threadIdx.x == 0) *out = s;
 }
 
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(256)
+k_compare(const typename VecOf<TA>::type* __restrict__ a, const typename VecOf<TB>::type* __restrict__ b,
+          uint64_t dim, double* __restrict__ partial)
+{
+    __shared__ double red[5][8];
+    double re = 0, im = 0, na = 0, nb = 0, mx = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += stride) {
+        const double ar = (double)a[i].x, ai = (double)a[i].y;
+        const double br = (double)b[i].x, bi = (double)b[i].y;
+        re += ar * br + ai * bi;            // conj(a) b
+        im += ar * bi - ai * br;
+        na += ar * ar + ai * ai;
+        nb += br * br + bi * bi;
+        const double dr = ar - br, di = ai - bi;
+        mx = fmax(mx, sqrt(dr * dr + di * di));
+    }
+    double v[5] = {re, im, na, nb, mx};
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        double x = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = (q == 4) ? fmax(x, y) : x + y;
+        }
+        if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        const int q = threadIdx.x;
+        double x = red[q][0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) x = (q == 4) ? fmax(x, red[q][w]) : x + red[q][w];
+        partial[(size_t)q * gridDim.x + blockIdx.x] = x;
+    }
+}
+
+__global__ void k_compare_final(const double* __restrict__ partial, int blocks, double* __restrict__ out)
+{
+    if (threadIdx.x != 0) return;
+    double v[5] = {0, 0, 0, 0, 0};
+    for (int q = 0; q < 5; q++)
+        for (int i = 0; i < blocks; i++) {
+            const double x = partial[(size_t)q * blocks + i];
+            v[q] = (q == 4) ? fmax(v[q], x) : v[q] + x;
+        }
+    for (int q = 0; q < 5; q++) out[q] = v[q];
+}
+
 }  // namespace
+
+template <typename TA, typename TB>
+cudaError_t compare_device(const void* a, const void* b, int n, double* d_out5, double* d_partial5,
+                           cudaStream_t s)
+{
+    const uint64_t dim = 1ull << n;
+    k_compare<TA, TB><<<REDUCE_BLOCKS, 256, 0, s>>>(static_cast<const typename VecOf<TA>::type*>(a),
+                                                   static_cast<const typename VecOf<TB>::type*>(b), dim,
+                                                   d_partial5);
+    k_compare_final<<<1, 32, 0, s>>>(d_partial5, REDUCE_BLOCKS, d_out5);
+    return cudaGetLastError();
+}
+template cudaError_t compare_device<double, double>(const void*, const void*, int, double*, double*, cudaStream_t);
+template cudaError_t compare_device<double, float>(const void*, const void*, int, double*, double*, cudaStream_t);
+template cudaError_t compare_device<float, double>(const void*, const void*, int, double*, double*, cudaStream_t);
+template cudaError_t compare_device<float, float>(const void*, const void*, int, double*, double*, cudaStream_t);
 
 size_t measure_scratch_doubles(int n)
 {

@@ -121,6 +121,55 @@ struct StagedPlan {
 void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& plan);
 
 // ---------------------------------------------------------------------------------
+// Fused tensor-core engine (FP32 states): passes of up to FT_MAX_BLOCKS fused k-qubit
+// blocks over tiles of 2^FT_TILE_BITS amplitudes (fuse.cpp, kernels_fused.cu)
+// ---------------------------------------------------------------------------------
+constexpr int FT_TILE_BITS = 12;     // 4096 FP32 amplitudes per tile (32 KiB)
+constexpr int FT_LOW_BITS = 4;       // the 4 lowest qubits are always local (128-byte runs)
+constexpr int FT_MAX_BLOCKS = 4;     // fused blocks per pass (shared-memory bound)
+constexpr int FT_THREADS = 128;      // one thread per TMEM lane
+constexpr int FT_MIN_K = 3, FT_MAX_K = 5;
+
+struct FusedBlock {                  // 752 bytes
+    uint16_t a_sc[64];               // target index a -> local index bits
+    uint16_t n_lo[32];               // row bits 0-4 -> local index bits
+    uint16_t n_hi[16];               // row bits 5-8 -> local index bits
+    uint32_t off_lo[64];             // local index bits 0-5 -> word offset in the state operand
+    uint32_t off_hi[64];             // local index bits 6-11 -> word offset
+    uint32_t gate_word;              // word offset of the gate operand (hi plane, then lo)
+    uint32_t pad[3];
+};
+static_assert(sizeof(FusedBlock) % 16 == 0, "FusedBlock layout");
+
+struct FusedPass {
+    uint8_t local_q[FT_TILE_BITS];
+    uint8_t nonlocal_q[64 - FT_TILE_BITS];
+    uint64_t g_lo[64];               // local index bits 0-5 -> global amplitude offset
+    uint64_t g_hi[64];               // local index bits 6-11 -> global amplitude offset
+    int32_t n_nonlocal, block_begin, n_blocks, pad;
+};
+static_assert(sizeof(FusedPass) % 16 == 0, "FusedPass layout");
+
+struct FusedPlan {
+    int k = 0;
+    std::vector<FusedPass> passes;
+    std::vector<FusedBlock> blocks;
+    std::vector<float> gates;        // per block: hi plane then lo plane, canonical layout
+};
+
+bool fusable(const std::vector<EOp>& ops);
+void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan);
+
+struct DevFusedBuffers {
+    FusedPass* passes = nullptr;
+    FusedBlock* blocks = nullptr;
+    float* gates = nullptr;
+    int* err = nullptr;
+};
+cudaError_t launch_fused_pass(void* state, int n, int k, int pass_index, int n_blocks,
+                              int gate_words_per_block, const DevFusedBuffers& b, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------
 // Kernel launchers (kernels_apply.cu)
 // ---------------------------------------------------------------------------------
 struct DevPlanBuffers {
@@ -167,6 +216,9 @@ template <typename T>
 cudaError_t expectation_device(const void* state, int n, const svb_pauli_term* d_terms,
                                int n_terms, double* d_out, double* d_partial, cudaStream_t s);
 constexpr int REDUCE_BLOCKS = 592;   // 4 x 148 SMs
+template <typename TA, typename TB>
+cudaError_t compare_device(const void* a, const void* b, int n, double* d_out5, double* d_partial5,
+                           cudaStream_t s);
 
 // ---------------------------------------------------------------------------------
 // Adjoint (adjoint.cu)
@@ -191,6 +243,8 @@ struct Sim {
     int engine = SVB_ENGINE_PER_GATE;
     StagedPlan staged;
     DevPlanBuffers dplan;
+    FusedPlan fused;
+    DevFusedBuffers dfused;
     bool have_circuit = false;
     cudaGraphExec_t graph = nullptr;
     cudaStream_t capture_stream = nullptr;

@@ -59,6 +59,7 @@ _SIGS = {
     "svb_expectation": ([_vp, _vp, ctypes.c_size_t, _dp], ctypes.c_int),
     "svb_adjoint": ([_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, _vp, ctypes.c_size_t, _dp, _dp],
                     ctypes.c_int),
+    "svb_compare_states": ([_vp, _vp, _dp, _dp], ctypes.c_int),
     "svb_last_error": ([], ctypes.c_char_p),
     "svb_version": ([], ctypes.c_char_p),
 }
@@ -171,6 +172,13 @@ class Handle:
         v = ctypes.c_double()
         check(lib().svb_expectation(self.ptr, t.ctypes.data, len(t), ctypes.byref(v)))
         return v.value
+
+    def compare(self, other: "Handle"):
+        """(fidelity, max |a_i - b_i|) against another handle's state, in FP64."""
+        f = ctypes.c_double()
+        d = ctypes.c_double()
+        check(lib().svb_compare_states(self.ptr, other.ptr, ctypes.byref(f), ctypes.byref(d)))
+        return f.value, d.value
 
     def adjoint(self, gates, bindings, n_params, terms):
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)

@@ -174,3 +174,82 @@ extern "C" int emu_plan_dump(uint32_t n, const svb_gate* gates, size_t n_gates, 
     fflush(stdout);
     return 0;
 }
+
+// ---- fused tensor-core plans ---------------------------------------------------------
+// Executes a fused plan on the CPU with the kernel's data flow: operand offsets from the
+// block tables, D[n][m'] = sum_kk X[n][kk] (G_hi + G_lo)[m'][kk] read through the
+// canonical K-major layout, rows scattered back through the a/n tables.  The MMA is
+// evaluated in FP64 here; only the layout and table logic are under test.
+static uint32_t emu_kmajor(uint32_t row, uint32_t kk, uint32_t rows)
+{
+    return ((kk >> 2) * (rows * 16u) + (row >> 3) * 128u + (row & 7u) * 16u + (kk & 3u) * 4u) / 4u;
+}
+
+extern "C" int emu_fused_run(uint32_t n, const svb_gate* gates, size_t n_gates, int k,
+                             double* re, double* im, uint64_t* n_passes, uint64_t* n_blocks)
+{
+    if ((int)n < FT_TILE_BITS || k < FT_MIN_K || k > FT_MAX_K) return -1;
+    std::vector<EOp> eops;
+    for (size_t i = 0; i < n_gates; i++)
+        if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
+    if (!fusable(eops)) return -3;
+    FusedPlan plan;
+    plan_fused(eops, (int)n, k, plan);
+    if (n_passes) *n_passes = plan.passes.size();
+    if (n_blocks) *n_blocks = plan.blocks.size();
+    const int N = 1 << (k + 1), ROWS = 1 << (FT_TILE_BITS - k);
+    const uint64_t tiles = 1ull << (n - FT_TILE_BITS);
+    std::vector<double> X(4096 * 2), Y(4096 * 2);
+    std::vector<double> tile_re(4096), tile_im(4096);
+    for (const FusedPass& P : plan.passes) {
+        for (uint64_t t = 0; t < tiles; t++) {
+            uint64_t base = 0;
+            for (int j = 0; j < P.n_nonlocal; j++) base |= ((t >> j) & 1ull) << P.nonlocal_q[j];
+            std::vector<int> seen(4096, 0);
+            for (uint32_t l = 0; l < 4096; l++) {
+                const uint64_t g = base + P.g_lo[l & 63] + P.g_hi[l >> 6];
+                const FusedBlock& B0 = plan.blocks[P.block_begin];
+                const uint32_t w = B0.off_lo[l & 63] + B0.off_hi[l >> 6];
+                if (w + 1 >= X.size() || seen[w / 2]++) return -2;
+                X[w] = re[g];
+                X[w + 1] = im[g];
+            }
+            for (int b = 0; b < P.n_blocks; b++) {
+                const FusedBlock& B = plan.blocks[P.block_begin + b];
+                const float* gh = plan.gates.data() + B.gate_word;
+                const float* gl = gh + (size_t)N * N;
+                for (int nrow = 0; nrow < ROWS; nrow++) {
+                    std::vector<double> d(N, 0.0);
+                    for (int mp = 0; mp < N; mp++) {
+                        double s = 0;
+                        for (int kk = 0; kk < N; kk++) {
+                            const uint32_t gw = emu_kmajor(mp, kk, N);
+                            s += X[emu_kmajor(nrow, kk, ROWS)] * ((double)gh[gw] + (double)gl[gw]);
+                        }
+                        d[mp] = s;
+                    }
+                    const uint32_t nl = B.n_lo[nrow & 31] | B.n_hi[nrow >> 5];
+                    for (int a = 0; a < (1 << k); a++) {
+                        const uint32_t l = nl | B.a_sc[a];
+                        if (b + 1 < P.n_blocks) {
+                            const FusedBlock& B1 = plan.blocks[P.block_begin + b + 1];
+                            const uint32_t w = B1.off_lo[l & 63] + B1.off_hi[l >> 6];
+                            Y[w] = d[2 * a];
+                            Y[w + 1] = d[2 * a + 1];
+                        } else {
+                            tile_re[l] = d[2 * a];
+                            tile_im[l] = d[2 * a + 1];
+                        }
+                    }
+                }
+                if (b + 1 < P.n_blocks) X.swap(Y);
+            }
+            for (uint32_t l = 0; l < 4096; l++) {
+                const uint64_t g = base + P.g_lo[l & 63] + P.g_hi[l >> 6];
+                re[g] = tile_re[l];
+                im[g] = tile_im[l];
+            }
+        }
+    }
+    return 0;
+}

@@ -102,3 +102,42 @@ def test_plan_pass_counts_headline_circuit(emu):
     assert rc == 0
     assert d.value == 1800
     assert a.value <= 80          # passes (each one read + one write of the state)
+
+
+def run_fused_emu(lib, n, gates, k):
+    re = np.zeros(1 << n)
+    im = np.zeros(1 << n)
+    re[0] = 1.0
+    a, b = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib.emu_fused_run(n, gates.ctypes.data, ctypes.c_size_t(len(gates)), k,
+                           re.ctypes.data_as(_dp), im.ctypes.data_as(_dp), ctypes.byref(a),
+                           ctypes.byref(b))
+    return rc, re, im, a.value, b.value
+
+
+@pytest.mark.parametrize("n,k", [(12, 5), (13, 4), (14, 3), (15, 5)])
+def test_fused_plan_random_matching(emu, oracle, n, k):
+    """Fusion into k-qubit blocks, operand layouts and index tables of the tensor-core
+    engine, executed on the CPU (MMA in FP64): only the FP32 rounding of the gates remains."""
+    g = circuits.random_matching_circuit(n, 6, seed=n * 7 + k)
+    rc, re, im, passes, blocks = run_fused_emu(emu, n, g, k)
+    assert rc == 0
+    ore, oim = oracle.run(n, g)
+    assert 1 - fidelity(re + 1j * im, ore + 1j * oim) < 1e-12
+    assert np.max(np.abs(re - ore)) < 1e-7 and blocks < len(g)
+
+
+def test_fused_plan_every_op_but_srn(emu, oracle):
+    n = 12
+    g = mixed_circuit(n, 3, seed=21)
+    g = g[g["op"] != G.OP["SRN"]]
+    rc, re, im, _, _ = run_fused_emu(emu, n, g, 4)
+    assert rc == 0
+    ore, oim = oracle.run(n, g)
+    assert 1 - fidelity(re + 1j * im, ore + 1j * oim) < 1e-12
+
+
+def test_fused_plan_rejects_srn(emu):
+    g = G.to_array([G.H(0), G.SRN(3)])
+    rc, *_ = run_fused_emu(emu, 12, g, 4)
+    assert rc == -3
