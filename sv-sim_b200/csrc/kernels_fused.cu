@@ -1,6 +1,8 @@
 // Fused tensor-core engine: tcgen05 MMAs on an FP32 state tile in shared memory.
 //
-// One persistent CTA per SM (4 warps = the 128 TMEM lanes) walks the tiles of a pass.
+// One persistent CTA per SM (8 warps, two per TMEM lane quadrant) walks the tiles of a
+// pass; the next tile is loaded into registers while the current one is in the tensor
+// core.
 // For a tile of 4096 amplitudes (12 local qubits) and a fused block on k target qubits,
 // the tile is viewed as X[n][kk]: rows n = the 2^(12-k) values of the other local
 // qubits, kk = 2a + re/im for the 2^k target values a.  The block's real-form gate
@@ -89,6 +91,18 @@ __device__ __forceinline__ float tf32_rna(float x)
     return __uint_as_float(r);
 }
 
+// 8 consecutive TMEM columns of this warp's 32 lanes
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v)
+{
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
+
 // 16 consecutive TMEM columns of this warp's 32 lanes
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
 {
@@ -138,8 +152,10 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
     constexpr int ROWS = 1 << (FT_TILE_BITS - K);   // rows of the state operand
     constexpr int MBLK = ROWS / 128;                // M = 128 blocks
     constexpr int KSTEPS = N / 8;                   // tf32 MMA K = 8
+    constexpr int HALF = N / 2;                     // TMEM columns read per thread and M block
     constexpr uint32_t GATE_WORDS = 2u * N * N;     // hi + lo planes
     constexpr uint32_t IDESC = umma_idesc_tf32(N);
+    constexpr int PAIRS = 4096 / 2 / FT_THREADS;    // float4 (2 amplitudes) per thread
     static_assert(MBLK * N <= (int)kTmemCols, "TMEM columns");
 
     extern __shared__ __align__(128) unsigned char sm[];
@@ -153,6 +169,8 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
+    const int quad = warp & 3;          // TMEM lane quadrant of this warp
+    const int half = warp >> 2;         // which half of the D columns it reads
 
     // -- stage the pass, its blocks and their gate operands in shared memory
     {
@@ -193,15 +211,40 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
     uint32_t parity = 0;
     bool ok = true;
 
-    for (uint64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    auto tile_base = [&](uint64_t tile) {
         uint64_t base = 0;
         for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
-        // load the tile (thread t owns local indices t + 128 j) into block 0's operand
-#pragma unroll 4
-        for (int j = 0; j < 32; j++) {
-            const uint32_t l = (uint32_t)tid + 128u * (uint32_t)j;
-            const float2 a = sv[base + P.g_lo[l & 63u] + P.g_hi[l >> 6]];
-            put_operand(xh, xl, sb[0], l, a.x, a.y);
+        return base;
+    };
+    // thread t owns the amplitude pairs at local indices 2 (t + 256 j), j < PAIRS; the
+    // lowest local qubit is global qubit 0, so each pair is 16 contiguous bytes
+    float4 cur[PAIRS];
+    uint64_t base = tile_base(blockIdx.x);
+    if (blockIdx.x < tiles) {
+#pragma unroll
+        for (int j = 0; j < PAIRS; j++) {
+            const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
+            cur[j] = *reinterpret_cast<const float4*>(sv + base + P.g_lo[l & 63u] + P.g_hi[l >> 6]);
+        }
+    }
+
+    for (uint64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        // block 0 operand from the registers
+#pragma unroll
+        for (int j = 0; j < PAIRS; j++) {
+            const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
+            put_operand(xh, xl, sb[0], l, cur[j].x, cur[j].y);
+            put_operand(xh, xl, sb[0], l + 1, cur[j].z, cur[j].w);
+        }
+        // prefetch the next tile while this one is in the tensor core
+        const uint64_t next = tile + gridDim.x;
+        const uint64_t nbase = next < tiles ? tile_base(next) : 0;
+        if (next < tiles) {
+#pragma unroll
+            for (int j = 0; j < PAIRS; j++) {
+                const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
+                cur[j] = *reinterpret_cast<const float4*>(sv + nbase + P.g_lo[l & 63u] + P.g_hi[l >> 6]);
+            }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -235,27 +278,33 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
             ok = __syncthreads_and(got ? 1 : 0) != 0;
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // this thread's D rows: n = 32 warp + lane + 128 mb
+            // this warp's D rows n = 32 quad + lane + 128 mb, columns of its half
             const FusedBlock& B = sb[b];
             const bool last = (b == nb - 1);
-            float2* stage = reinterpret_cast<float2*>(xh);     // plain tile copy after the last block
-            float dv[MBLK][N];
+            float dv[MBLK][HALF];
 #pragma unroll
-            for (int mb = 0; mb < MBLK; mb++)
+            for (int mb = 0; mb < MBLK; mb++) {
+                const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(mb * N + half * HALF);
+                if constexpr (HALF >= 16) {
 #pragma unroll
-                for (int c = 0; c < N; c += 16)
-                    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mb * N + c), &dv[mb][c]);
+                    for (int c = 0; c < HALF; c += 16) tmem_ld16(ta + (uint32_t)c, &dv[mb][c]);
+                } else {
+                    tmem_ld8(ta, &dv[mb][0]);
+                }
+            }
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();   // every row is read before the operand planes are overwritten
+            float2* stage = reinterpret_cast<float2*>(xh);     // plain tile copy after the last block
 #pragma unroll
             for (int mb = 0; mb < MBLK; mb++) {
-                const uint32_t n = (uint32_t)(warp * 32 + (tid & 31) + 128 * mb);
+                const uint32_t n = (uint32_t)(quad * 32 + (tid & 31) + 128 * mb);
                 const uint32_t nl = B.n_lo[n & 31u] | B.n_hi[n >> 5];
 #pragma unroll
-                for (int a = 0; a < (1 << K); a++) {
+                for (int a2 = 0; a2 < HALF / 2; a2++) {
+                    const int a = half * (HALF / 2) + a2;
                     const uint32_t l = nl | B.a_sc[a];
-                    const float re = dv[mb][2 * a], im = dv[mb][2 * a + 1];
+                    const float re = dv[mb][2 * a2], im = dv[mb][2 * a2 + 1];
                     if (last) stage[l] = make_float2(re, im);
                     else put_operand(xh, xl, sb[b + 1], l, re, im);
                 }
@@ -265,15 +314,19 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
         }
         if (!ok) break;
         // store the tile
-        const float2* stage = reinterpret_cast<const float2*>(xh);
-#pragma unroll 4
-        for (int j = 0; j < 32; j++) {
-            const uint32_t l = (uint32_t)tid + 128u * (uint32_t)j;
-            sv[base + P.g_lo[l & 63u] + P.g_hi[l >> 6]] = stage[l];
+        const float4* stage4 = reinterpret_cast<const float4*>(xh);
+#pragma unroll
+        for (int j = 0; j < PAIRS; j++) {
+            const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
+            *reinterpret_cast<float4*>(sv + base + P.g_lo[l & 63u] + P.g_hi[l >> 6]) = stage4[l >> 1];
         }
+        base = nbase;
         __syncthreads();
     }
-    if (!ok && tid == 0) atomicExch(err, 1);
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+        mbar_wait(bar, parity ^ 1u);     // bounded: let an MMA still in flight finish
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)

@@ -127,7 +127,7 @@ void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& p
 constexpr int FT_TILE_BITS = 12;     // 4096 FP32 amplitudes per tile (32 KiB)
 constexpr int FT_LOW_BITS = 4;       // the 4 lowest qubits are always local (128-byte runs)
 constexpr int FT_MAX_BLOCKS = 4;     // fused blocks per pass (shared-memory bound)
-constexpr int FT_THREADS = 128;      // one thread per TMEM lane
+constexpr int FT_THREADS = 256;      // two warps per TMEM lane quadrant
 constexpr int FT_MIN_K = 3, FT_MAX_K = 5;
 
 struct FusedBlock {                  // 752 bytes
