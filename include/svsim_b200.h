@@ -156,6 +156,27 @@ svb_status svb_state_device_ptr(svb_sim* sim, void** dptr, int* precision);
 svb_status svb_measure(svb_sim* sim, const double* uniforms, uint32_t shots,
                        uint64_t* out, double* prob_total);
 
+/* Largest state size svb_measure_noalloc accepts. */
+#define SVB_NOALLOC_MAX_QUBITS 30
+
+/* Measurement that allocates nothing (no counterpart in the reference).  Same sampling
+ * rule and results as svb_measure, for callers that cannot allocate device memory: an
+ * application whose device memory is fully reserved by its own pool, or one that owns
+ * the state buffer and wants no hidden cudaMalloc/cudaFree.  Every pointer is a device
+ * pointer on the current device: `state` (2^n_qubits interleaved amplitudes of
+ * `precision`), `uniforms` and `samples` (`shots` entries each) and `prob_total` (one
+ * double, may be NULL).  Work is queued on `stream`; results are valid once it completes.
+ * The FP64 scratch lives in a fixed array of about 4 MiB in the library's device image,
+ * sized for n_qubits <= SVB_NOALLOC_MAX_QUBITS; larger states are rejected with
+ * SVB_ERR_INVALID.  The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.  All calls
+ * on a device share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller.  Nothing needs clearing between calls (the kernels overwrite what they
+ * read). */
+svb_status svb_measure_noalloc(const void* state, uint32_t n_qubits, int precision,
+                               const double* uniforms, uint32_t shots, uint64_t* samples,
+                               double* prob_total, void* stream);
+
 /* Squared norm sum |a|^2 in FP64 (the value the reference checks against 1 at :379). */
 svb_status svb_norm2(svb_sim* sim, double* out);
 
