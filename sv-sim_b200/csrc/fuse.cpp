@@ -157,9 +157,10 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
         P.block_begin = (int32_t)plan.blocks.size();
 
         // -- blocks: up to k qubits each, commuting ops pulled forward
+        struct BlockOps { std::vector<int> tq; std::vector<int> ops; };
+        std::vector<BlockOps> pblocks;
         remaining = taken;
-        int nblocks = 0;
-        while (!remaining.empty() && nblocks < FT_MAX_BLOCKS) {
+        while (!remaining.empty() && (int)pblocks.size() < fused_max_blocks(k)) {
             uint64_t S = 0;
             uint64_t blk_blocked = 0;
             blk.clear();
@@ -183,67 +184,93 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
                 const int q = P.local_q[p];
                 if (!((S >> q) & 1)) { tq.push_back(q); S |= bit(q); }
             }
-            std::sort(tq.begin(), tq.end());
+            pblocks.push_back({tq, blk});
+            remaining.swap(rest);
+        }
+        const int nblocks = (int)pblocks.size();
+
+        // Bit orderings.  The threads that write block f's operand have lane bits 0..3 on
+        // the local positions W_f (the tile loader's positions 1..4 for f = 0, otherwise
+        // row bits 0..3 of block f-1).  Their 8-byte stores are conflict-free when W_f lands
+        // on {target bit 0, row bits 0..2} of block f, so those come first.
+        std::vector<std::vector<int>> T(nblocks), C(nblocks);
+        std::vector<int> W = {1, 2, 3, 4};
+        for (int f = 0; f < nblocks; f++) {
+            uint32_t tmask = 0;
+            for (int q : pblocks[f].tq) tmask |= 1u << pos_of[q];
+            std::vector<int>& t = T[f];
+            std::vector<int>& c = C[f];
+            for (int p : W)
+                if (((tmask >> p) & 1) && t.empty()) t.push_back(p);
+            for (int p = 0; p < M; p++)
+                if (((tmask >> p) & 1) && std::find(t.begin(), t.end(), p) == t.end()) t.push_back(p);
+            for (int p : W)
+                if (!((tmask >> p) & 1)) c.push_back(p);
+            for (int p = 0; p < M; p++)
+                if (!((tmask >> p) & 1) && std::find(c.begin(), c.end(), p) == c.end()) c.push_back(p);
+            W.assign(c.begin(), c.begin() + 4);
+        }
+
+        // per-block tables; offsets are additive over disjoint bit groups of the local index
+        auto operand_word = [&](int f, uint32_t l) -> uint32_t {
+            uint32_t row = 0, a = 0;
+            for (int i = 0; i < k; i++)
+                if ((l >> T[f][i]) & 1) a |= 1u << i;
+            for (size_t i = 0; i < C[f].size(); i++)
+                if ((l >> C[f][i]) & 1) row |= 1u << i;
+            return kmajor_offset(row, 2 * a, rows) / 4;
+        };
+        std::vector<FusedBlock> fb(nblocks);
+        for (int f = 0; f < nblocks; f++) {
+            FusedBlock& B = fb[f];
+            std::memset(&B, 0, sizeof(B));
+            for (int a = 0; a < 64; a++) {
+                uint32_t l = 0;
+                for (int i = 0; i < k; i++)
+                    if ((a >> i) & 1) l |= 1u << T[f][i];
+                B.a_sc[a] = (uint16_t)(a < (1 << k) ? l : 0);
+            }
+            for (int j = 0; j < 32; j++) {
+                uint32_t l = 0;
+                for (int i = 0; i < 5 && i < (int)C[f].size(); i++)
+                    if ((j >> i) & 1) l |= 1u << C[f][i];
+                B.n_lo[j] = (uint16_t)l;
+            }
+            for (int j = 0; j < 16; j++) {
+                uint32_t l = 0;
+                for (int i = 0; i < 4 && 5 + i < (int)C[f].size(); i++)
+                    if ((j >> i) & 1) l |= 1u << C[f][5 + i];
+                B.n_hi[j] = (uint16_t)l;
+            }
+            for (int j = 0; j < 64; j++) {
+                B.off_lo[j] = operand_word(f, (uint32_t)j);
+                B.off_hi[j] = operand_word(f, (uint32_t)j << 6);
+            }
+        }
+        for (int f = 0; f < nblocks; f++) {
+            FusedBlock& B = fb[f];
+            const bool last = (f == nblocks - 1);
+            auto nxt = [&](uint32_t l) -> uint32_t { return last ? l : operand_word(f + 1, l); };
+            for (int a = 0; a < 64; a++) B.nxt_a[a] = nxt(B.a_sc[a]);
+            for (int j = 0; j < 32; j++) B.nxt_nlo[j] = nxt(B.n_lo[j]);
+            for (int j = 0; j < 16; j++) B.nxt_nhi[j] = nxt(B.n_hi[j]);
+        }
+
+        // block matrices: gate operand B[m'][kk] for the real form, hi and lo planes
+        for (int f = 0; f < nblocks; f++) {
+            // qubit -> bit of the block's matrix index, in the order of T[f]
             int tpos[64];
             for (int q = 0; q < 64; q++) tpos[q] = -1;
-            for (int i = 0; i < k; i++) tpos[tq[i]] = i;
-            // the block matrix, column by column
+            for (int i = 0; i < k; i++) tpos[P.local_q[T[f][i]]] = i;
             const int d = 1 << k;
             std::vector<cplx> U((size_t)d * d), col(d);
             for (int c = 0; c < d; c++) {
                 std::fill(col.begin(), col.end(), cplx(0, 0));
                 col[c] = 1.0;
-                for (int i : blk) apply_small(ops[i], tpos, col);
+                for (int i : pblocks[f].ops) apply_small(ops[i], tpos, col);
                 for (int r = 0; r < d; r++) U[(size_t)r * d + c] = col[r];
             }
-            // device block: index tables and gate operand
-            FusedBlock B;
-            std::memset(&B, 0, sizeof(B));
-            uint32_t tmask_pos = 0;
-            int tposl[8];
-            for (int i = 0; i < k; i++) { tposl[i] = pos_of[tq[i]]; tmask_pos |= 1u << tposl[i]; }
-            std::vector<int> cpos;
-            for (int p = 0; p < M; p++)
-                if (!((tmask_pos >> p) & 1)) cpos.push_back(p);
-            for (int a = 0; a < 64; a++) {
-                uint32_t l = 0;
-                for (int i = 0; i < k; i++)
-                    if ((a >> i) & 1) l |= 1u << tposl[i];
-                B.a_sc[a] = (uint16_t)l;
-            }
-            for (int j = 0; j < 32; j++) {
-                uint32_t l = 0;
-                for (int i = 0; i < 5 && i < (int)cpos.size(); i++)
-                    if ((j >> i) & 1) l |= 1u << cpos[i];
-                B.n_lo[j] = (uint16_t)l;
-            }
-            for (int j = 0; j < 16; j++) {
-                uint32_t l = 0;
-                for (int i = 0; i < 4 && 5 + i < (int)cpos.size(); i++)
-                    if ((j >> i) & 1) l |= 1u << cpos[5 + i];
-                B.n_hi[j] = (uint16_t)l;
-            }
-            // word offsets (of the real part) in this block's state operand, additive over
-            // the 6-bit halves of the local index
-            for (int half = 0; half < 2; half++) {
-                for (int j = 0; j < 64; j++) {
-                    uint32_t row = 0, a = 0;
-                    for (int b = 0; b < 6; b++) {
-                        if (!((j >> b) & 1)) continue;
-                        const int p = half * 6 + b;
-                        if ((tmask_pos >> p) & 1) {
-                            for (int i = 0; i < k; i++)
-                                if (tposl[i] == p) a |= 1u << i;
-                        } else {
-                            for (size_t i = 0; i < cpos.size(); i++)
-                                if (cpos[i] == p) row |= 1u << i;
-                        }
-                    }
-                    const uint32_t off = kmajor_offset(row, 2 * a, rows) / 4;
-                    if (half == 0) B.off_lo[j] = off; else B.off_hi[j] = off;
-                }
-            }
-            // gate operand: B[m'][kk] for the real form, hi and lo planes
+            FusedBlock& B = fb[f];
             const size_t plane = (size_t)N * N;
             B.gate_word = (uint32_t)plan.gates.size();
             plan.gates.resize(plan.gates.size() + 2 * plane);
@@ -257,18 +284,16 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
                     double val;
                     if (cr == 0) val = cc == 0 ? u.real() : -u.imag();
                     else val = cc == 0 ? u.imag() : u.real();
-                    const float f = (float)val;
-                    const float h = tf32_hi(f);
+                    const float fv = (float)val;
+                    const float h = tf32_hi(fv);
                     const uint32_t w = kmajor_offset(mp, kk, N) / 4;
                     hi[w] = h;
-                    lo[w] = f - h;
+                    lo[w] = fv - h;
                 }
             }
             plan.blocks.push_back(B);
-            nblocks++;
-            remaining.swap(rest);
         }
-        for (int i : remaining) done[i] = 0;   // did not fit in FT_MAX_BLOCKS blocks
+        for (int i : remaining) done[i] = 0;   // did not fit in this pass's blocks
         P.n_blocks = nblocks;
         plan.passes.push_back(P);
     }

@@ -117,33 +117,34 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+template <int K>
 struct FusedSmem {
     static constexpr uint32_t x_bytes = 4096u * 2u * 4u;                  // one plane: 32 KiB
-    static constexpr uint32_t gate_bytes_max = 2u * 64u * 64u * 4u;       // hi+lo for k = 5
+    static constexpr uint32_t n_real = 1u << (K + 1);
+    static constexpr uint32_t gate_bytes = 2u * n_real * n_real * 4u;     // hi + lo planes
+    static constexpr uint32_t max_blocks = (uint32_t)fused_max_blocks(K);
     static constexpr uint32_t x_hi = 0;
     static constexpr uint32_t x_lo = x_hi + x_bytes;
     static constexpr uint32_t gates = x_lo + x_bytes;
-    static constexpr uint32_t blocks = gates + FT_MAX_BLOCKS * gate_bytes_max;
-    static constexpr uint32_t pass = blocks + FT_MAX_BLOCKS * sizeof(FusedBlock);
+    static constexpr uint32_t blocks = gates + max_blocks * gate_bytes;
+    static constexpr uint32_t pass = blocks + max_blocks * sizeof(FusedBlock);
     static constexpr uint32_t misc = pass + sizeof(FusedPass);
     static constexpr uint32_t total = misc + 64;
+    static constexpr int ctas_per_sm = total <= 113u * 1024u ? 2 : 1;
     static_assert(gates % 16 == 0 && blocks % 16 == 0 && pass % 16 == 0 && misc % 16 == 0, "align");
 };
 
-// Writes amplitude (re, im) of local index l into the state operand of block B.
-__device__ __forceinline__ void put_operand(float* xh, float* xl, const FusedBlock& B, uint32_t l,
-                                            float re, float im)
+// Writes amplitude (re, im) at word offset w of the state operand (re and im are adjacent
+// K values, 8-byte aligned), split into the TF32 hi plane and the FP32 remainder plane.
+__device__ __forceinline__ void put_operand(float* xh, float* xl, uint32_t w, float re, float im)
 {
-    const uint32_t w = B.off_lo[l & 63u] + B.off_hi[l >> 6];
     const float hr = tf32_rna(re), hi = tf32_rna(im);
-    xh[w] = hr;
-    xh[w + 1] = hi;
-    xl[w] = re - hr;
-    xl[w + 1] = im - hi;
+    *reinterpret_cast<float2*>(xh + w) = make_float2(hr, hi);
+    *reinterpret_cast<float2*>(xl + w) = make_float2(re - hr, im - hi);
 }
 
 template <int K>
-__global__ void __launch_bounds__(FT_THREADS, 1)
+__global__ void __launch_bounds__(FT_THREADS, FusedSmem<K>::ctas_per_sm)
 k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
         const FusedBlock* __restrict__ blocks, const float* __restrict__ gates, int pass_index,
         uint64_t tiles, int* __restrict__ err)
@@ -159,13 +160,14 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
     static_assert(MBLK * N <= (int)kTmemCols, "TMEM columns");
 
     extern __shared__ __align__(128) unsigned char sm[];
-    float* xh = reinterpret_cast<float*>(sm + FusedSmem::x_hi);
-    float* xl = reinterpret_cast<float*>(sm + FusedSmem::x_lo);
-    float* sg = reinterpret_cast<float*>(sm + FusedSmem::gates);
-    FusedBlock* sb = reinterpret_cast<FusedBlock*>(sm + FusedSmem::blocks);
-    FusedPass* sp = reinterpret_cast<FusedPass*>(sm + FusedSmem::pass);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + FusedSmem::misc);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + FusedSmem::misc + 16);
+    using L = FusedSmem<K>;
+    float* xh = reinterpret_cast<float*>(sm + L::x_hi);
+    float* xl = reinterpret_cast<float*>(sm + L::x_lo);
+    float* sg = reinterpret_cast<float*>(sm + L::gates);
+    FusedBlock* sb = reinterpret_cast<FusedBlock*>(sm + L::blocks);
+    FusedPass* sp = reinterpret_cast<FusedPass*>(sm + L::pass);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::misc);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::misc + 16);
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -217,34 +219,37 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
         return base;
     };
     // thread t owns the amplitude pairs at local indices 2 (t + 256 j), j < PAIRS; the
-    // lowest local qubit is global qubit 0, so each pair is 16 contiguous bytes
+    // lowest local qubit is global qubit 0, so each pair is 16 contiguous bytes.  Their
+    // global offsets and their places in block 0's operand are fixed for the pass.
+    uint64_t gof[PAIRS];
+    uint32_t w0[PAIRS][2];
+#pragma unroll
+    for (int j = 0; j < PAIRS; j++) {
+        const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
+        gof[j] = P.g_lo[l & 63u] + P.g_hi[l >> 6];
+        w0[j][0] = sb[0].off_lo[l & 63u] + sb[0].off_hi[l >> 6];
+        w0[j][1] = sb[0].off_lo[(l + 1) & 63u] + sb[0].off_hi[(l + 1) >> 6];
+    }
     float4 cur[PAIRS];
     uint64_t base = tile_base(blockIdx.x);
     if (blockIdx.x < tiles) {
 #pragma unroll
-        for (int j = 0; j < PAIRS; j++) {
-            const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
-            cur[j] = *reinterpret_cast<const float4*>(sv + base + P.g_lo[l & 63u] + P.g_hi[l >> 6]);
-        }
+        for (int j = 0; j < PAIRS; j++) cur[j] = *reinterpret_cast<const float4*>(sv + base + gof[j]);
     }
 
     for (uint64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         // block 0 operand from the registers
 #pragma unroll
         for (int j = 0; j < PAIRS; j++) {
-            const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
-            put_operand(xh, xl, sb[0], l, cur[j].x, cur[j].y);
-            put_operand(xh, xl, sb[0], l + 1, cur[j].z, cur[j].w);
+            put_operand(xh, xl, w0[j][0], cur[j].x, cur[j].y);
+            put_operand(xh, xl, w0[j][1], cur[j].z, cur[j].w);
         }
         // prefetch the next tile while this one is in the tensor core
         const uint64_t next = tile + gridDim.x;
         const uint64_t nbase = next < tiles ? tile_base(next) : 0;
         if (next < tiles) {
 #pragma unroll
-            for (int j = 0; j < PAIRS; j++) {
-                const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
-                cur[j] = *reinterpret_cast<const float4*>(sv + nbase + P.g_lo[l & 63u] + P.g_hi[l >> 6]);
-            }
+            for (int j = 0; j < PAIRS; j++) cur[j] = *reinterpret_cast<const float4*>(sv + nbase + gof[j]);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -299,14 +304,14 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
 #pragma unroll
             for (int mb = 0; mb < MBLK; mb++) {
                 const uint32_t n = (uint32_t)(quad * 32 + (tid & 31) + 128 * mb);
-                const uint32_t nl = B.n_lo[n & 31u] | B.n_hi[n >> 5];
+                const uint32_t wn = B.nxt_nlo[n & 31u] + B.nxt_nhi[n >> 5];
 #pragma unroll
                 for (int a2 = 0; a2 < HALF / 2; a2++) {
                     const int a = half * (HALF / 2) + a2;
-                    const uint32_t l = nl | B.a_sc[a];
+                    const uint32_t w = wn + B.nxt_a[a];
                     const float re = dv[mb][2 * a2], im = dv[mb][2 * a2 + 1];
-                    if (last) stage[l] = make_float2(re, im);
-                    else put_operand(xh, xl, sb[b + 1], l, re, im);
+                    if (last) stage[w] = make_float2(re, im);
+                    else put_operand(xh, xl, w, re, im);
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -316,10 +321,8 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
         // store the tile
         const float4* stage4 = reinterpret_cast<const float4*>(xh);
 #pragma unroll
-        for (int j = 0; j < PAIRS; j++) {
-            const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
-            *reinterpret_cast<float4*>(sv + base + P.g_lo[l & 63u] + P.g_hi[l >> 6]) = stage4[l >> 1];
-        }
+        for (int j = 0; j < PAIRS; j++)
+            *reinterpret_cast<float4*>(sv + base + gof[j]) = stage4[tid + FT_THREADS * j];
         base = nbase;
         __syncthreads();
     }
@@ -337,19 +340,25 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
 template <int K>
 cudaError_t launch_k(void* state, int n, int pass_index, const DevFusedBuffers& b, cudaStream_t s)
 {
-    static int sms[64] = {0};
+    static int ctas[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 64 && sms[dev] == 0) {
+    if (dev >= 64) return cudaErrorInvalidDevice;
+    if (ctas[dev] == 0) {
         cudaError_t e = cudaFuncSetAttribute(k_fused<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)FusedSmem::total);
+                                             (int)FusedSmem<K>::total);
         if (e != cudaSuccess) return e;
-        e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        int sms = 0, per_sm = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<K>, FT_THREADS,
+                                                          FusedSmem<K>::total);
+        if (e != cudaSuccess) return e;
+        ctas[dev] = sms * (per_sm > 0 ? per_sm : 1);
     }
     const uint64_t tiles = 1ull << (n - FT_TILE_BITS);
-    const uint64_t grid = tiles < (uint64_t)sms[dev] ? tiles : (uint64_t)sms[dev];
-    k_fused<K><<<(unsigned)grid, FT_THREADS, FusedSmem::total, s>>>(
+    const uint64_t grid = tiles < (uint64_t)ctas[dev] ? tiles : (uint64_t)ctas[dev];
+    k_fused<K><<<(unsigned)grid, FT_THREADS, FusedSmem<K>::total, s>>>(
         static_cast<float2*>(state), b.passes, b.blocks, b.gates, pass_index, tiles, b.err);
     return cudaGetLastError();
 }

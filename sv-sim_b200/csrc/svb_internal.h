@@ -126,16 +126,25 @@ void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& p
 // ---------------------------------------------------------------------------------
 constexpr int FT_TILE_BITS = 12;     // 4096 FP32 amplitudes per tile (32 KiB)
 constexpr int FT_LOW_BITS = 4;       // the 4 lowest qubits are always local (128-byte runs)
-constexpr int FT_MAX_BLOCKS = 4;     // fused blocks per pass (shared-memory bound)
+constexpr int FT_MAX_BLOCKS = 8;     // upper bound of fused blocks per pass
+// blocks per pass that fit in shared memory: k = 5 keeps one CTA per SM (4 gate
+// operands of 32 KiB); k <= 4 leaves room for two CTAs per SM
+__host__ __device__ constexpr int fused_max_blocks(int k) { return k >= 5 ? 4 : (k == 4 ? 5 : 8); }
 constexpr int FT_THREADS = 256;      // two warps per TMEM lane quadrant
 constexpr int FT_MIN_K = 3, FT_MAX_K = 5;
 
-struct FusedBlock {                  // 752 bytes
+struct FusedBlock {                  // 1200 bytes
     uint16_t a_sc[64];               // target index a -> local index bits
     uint16_t n_lo[32];               // row bits 0-4 -> local index bits
     uint16_t n_hi[16];               // row bits 5-8 -> local index bits
     uint32_t off_lo[64];             // local index bits 0-5 -> word offset in the state operand
     uint32_t off_hi[64];             // local index bits 6-11 -> word offset
+    // where the amplitudes of this block's output rows go next: the word offset in the
+    // next block's operand, or (last block) the amplitude index in the plain tile copy;
+    // additive over the disjoint bit groups of the local index
+    uint32_t nxt_a[64];              // target index a
+    uint32_t nxt_nlo[32];            // row bits 0-4
+    uint32_t nxt_nhi[16];            // row bits 5-8
     uint32_t gate_word;              // word offset of the gate operand (hi plane, then lo)
     uint32_t pad[3];
 };

@@ -228,17 +228,20 @@ extern "C" int emu_fused_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
                         }
                         d[mp] = s;
                     }
+                    // the kernel's scatter: additive next-offset tables
+                    const uint32_t wn = B.nxt_nlo[nrow & 31] + B.nxt_nhi[nrow >> 5];
                     const uint32_t nl = B.n_lo[nrow & 31] | B.n_hi[nrow >> 5];
                     for (int a = 0; a < (1 << k); a++) {
-                        const uint32_t l = nl | B.a_sc[a];
+                        const uint32_t w = wn + B.nxt_a[a];
                         if (b + 1 < P.n_blocks) {
                             const FusedBlock& B1 = plan.blocks[P.block_begin + b + 1];
-                            const uint32_t w = B1.off_lo[l & 63] + B1.off_hi[l >> 6];
+                            const uint32_t l = nl | B.a_sc[a];
+                            if (w != B1.off_lo[l & 63] + B1.off_hi[l >> 6]) return -4;
                             Y[w] = d[2 * a];
                             Y[w + 1] = d[2 * a + 1];
                         } else {
-                            tile_re[l] = d[2 * a];
-                            tile_im[l] = d[2 * a + 1];
+                            tile_re[w] = d[2 * a];
+                            tile_im[w] = d[2 * a + 1];
                         }
                     }
                 }
