@@ -202,6 +202,50 @@ svb_status svb_adjoint(svb_sim* sim, const svb_gate* gates, const svb_param_bind
                        size_t n_gates, uint32_t n_params, const svb_pauli_term* terms,
                        size_t n_terms, double* energy, double* grad);
 
+/* ---- batched QAOA (no reference counterpart) ------------------------------------ */
+
+/* A batch of weighted MaxCut QAOA instances evaluated together: for each instance the
+ * cost expectation E = <psi|C|psi> and its gradient with respect to the 2p angles.
+ * Instance i has n_qubits[i] qubits and the edges edge_offsets[i] .. edge_offsets[i+1]-1
+ * of `edges` (pairs a, b) with `weights`.  Its circuit is what the reference builds from
+ * H on every qubit, then per layer l RZZ(-gamma_l w_e) on every edge (:1288-1294) and
+ * RX(2 beta_l) on every qubit (:1085-1100); C(z) = sum_e w_e [z_a != z_b]. */
+typedef struct svb_qaoa_batch svb_qaoa_batch;
+
+typedef struct {
+    uint32_t n_instances;
+    uint32_t p;
+    uint32_t tile_bits;          /* log2 amplitudes per tile of the batched kernel */
+    uint32_t graphed;            /* 1 if svb_qaoa_run replays a CUDA graph */
+    uint64_t total_amplitudes;   /* sum over instances of 2^n */
+    uint64_t tiles_per_pass;
+    double moved_bytes;          /* state and cost-table bytes one evaluation reads and writes */
+    uint32_t grid;               /* resident blocks of the persistent launch */
+    uint32_t reserved;
+} svb_qaoa_stats;
+
+/* Builds the batch on `device`: uploads the graphs, computes every instance's cost
+ * table and captures one evaluation (parameters in, one cooperative launch, results
+ * out) as a CUDA graph.  Each instance has 2 <= n <= 24 qubits (FP64) or 26 (FP32) and at
+ * most 512 edges; edge_offsets has n_instances + 1 entries starting at 0. */
+svb_status svb_qaoa_create(int device, int precision, uint32_t n_instances, const uint32_t* n_qubits,
+                           const uint32_t* edge_offsets, const uint32_t* edges, const double* weights,
+                           uint32_t p, svb_qaoa_batch** out);
+
+/* One evaluation at gammas[i*p + l], betas[i*p + l] (host arrays).  Writes energies[i]
+ * and grads[i*2p + l] = dE_i/dgamma_l, grads[i*2p + p + l] = dE_i/dbeta_l (either may be
+ * NULL).  Blocks until the results are on the host. */
+svb_status svb_qaoa_run(svb_qaoa_batch* batch, const double* gammas, const double* betas,
+                        double* energies, double* grads);
+
+/* Queues the evaluation kernel alone on `stream`, with the parameters of the last
+ * svb_qaoa_run and results left on the device (for timing the kernel by itself). */
+svb_status svb_qaoa_launch(svb_qaoa_batch* batch, void* stream);
+
+svb_status svb_qaoa_info(const svb_qaoa_batch* batch, svb_qaoa_stats* info);
+
+svb_status svb_qaoa_destroy(svb_qaoa_batch* batch);
+
 /* ---- diagnostics ---------------------------------------------------------------- */
 
 /* Message of the last failed call on this thread ("" if none). */

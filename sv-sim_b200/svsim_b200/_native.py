@@ -35,6 +35,14 @@ class PlanInfo(ctypes.Structure):
                 ("tile_bits", ctypes.c_int)]
 
 
+class QaoaStats(ctypes.Structure):
+    _fields_ = [("n_instances", ctypes.c_uint32), ("p", ctypes.c_uint32),
+                ("tile_bits", ctypes.c_uint32), ("graphed", ctypes.c_uint32),
+                ("total_amplitudes", ctypes.c_uint64), ("tiles_per_pass", ctypes.c_uint64),
+                ("moved_bytes", ctypes.c_double), ("grid", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
 _lib = None
 
 _vp = ctypes.c_void_p
@@ -60,6 +68,12 @@ _SIGS = {
     "svb_adjoint": ([_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, _vp, ctypes.c_size_t, _dp, _dp],
                     ctypes.c_int),
     "svb_compare_states": ([_vp, _vp, _dp, _dp], ctypes.c_int),
+    "svb_qaoa_create": ([ctypes.c_int, ctypes.c_int, ctypes.c_uint32, _vp, _vp, _vp, _vp, ctypes.c_uint32,
+                         ctypes.POINTER(_vp)], ctypes.c_int),
+    "svb_qaoa_run": ([_vp, _dp, _dp, _dp, _dp], ctypes.c_int),
+    "svb_qaoa_launch": ([_vp, _vp], ctypes.c_int),
+    "svb_qaoa_info": ([_vp, ctypes.POINTER(QaoaStats)], ctypes.c_int),
+    "svb_qaoa_destroy": ([_vp], ctypes.c_int),
     "svb_last_error": ([], ctypes.c_char_p),
     "svb_version": ([], ctypes.c_char_p),
 }
@@ -189,3 +203,54 @@ class Handle:
         check(lib().svb_adjoint(self.ptr, g.ctypes.data, b.ctypes.data, len(g), n_params,
                                 t.ctypes.data, len(t), ctypes.byref(e), dptr(grad)))
         return e.value, grad[:n_params]
+
+
+class QaoaBatch:
+    """A batch of MaxCut QAOA instances (svb_qaoa_create): energy and gradient of every
+    instance per call of ``run``."""
+
+    def __init__(self, instances, device: int = 0, precision: int = SVB_FP64):
+        ps = {len(inst.gammas) for inst in instances}
+        if len(ps) != 1:
+            raise ValueError("all instances of a batch need the same depth p")
+        self.p = ps.pop()
+        self.n_inst = len(instances)
+        nq = np.array([inst.n for inst in instances], dtype=np.uint32)
+        counts = np.array([len(inst.edges) for inst in instances], dtype=np.uint32)
+        eoff = np.zeros(self.n_inst + 1, dtype=np.uint32)
+        np.cumsum(counts, out=eoff[1:])
+        edges = np.ascontiguousarray(np.concatenate([np.asarray(i.edges, dtype=np.uint32).reshape(-1, 2)
+                                                     for i in instances]), dtype=np.uint32)
+        w = np.ascontiguousarray(np.concatenate([np.asarray(i.weights, dtype=np.float64)
+                                                 for i in instances]))
+        self.ptr = _vp()
+        check(lib().svb_qaoa_create(device, precision, self.n_inst, nq.ctypes.data, eoff.ctypes.data,
+                                    edges.ctypes.data, w.ctypes.data, self.p, ctypes.byref(self.ptr)))
+
+    def close(self):
+        if self.ptr:
+            lib().svb_qaoa_destroy(self.ptr)
+            self.ptr = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, gammas, betas):
+        """gammas, betas: [n_instances, p].  Returns (energies [n], grads [n, 2p])."""
+        g = np.ascontiguousarray(gammas, dtype=np.float64).reshape(self.n_inst, self.p)
+        b = np.ascontiguousarray(betas, dtype=np.float64).reshape(self.n_inst, self.p)
+        e = np.zeros(self.n_inst)
+        gr = np.zeros((self.n_inst, 2 * self.p))
+        check(lib().svb_qaoa_run(self.ptr, dptr(g), dptr(b), dptr(e), dptr(gr)))
+        return e, gr
+
+    def launch(self, stream: int = 0):
+        check(lib().svb_qaoa_launch(self.ptr, _vp(stream)))
+
+    def info(self) -> QaoaStats:
+        st = QaoaStats()
+        check(lib().svb_qaoa_info(self.ptr, ctypes.byref(st)))
+        return st

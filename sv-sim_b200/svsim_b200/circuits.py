@@ -145,6 +145,34 @@ class QaoaInstance:
                 rows.append((OP["RX"], (q, 0, 0, 0, 0), 2.0 * b, 0.0, 0.0))
         return _pack(rows)
 
+    def param_circuit(self) -> ParamCircuit:
+        """`circuit()` with its angles bound to params = [gamma_0..gamma_{p-1},
+        beta_0..beta_{p-1}] (RZZ theta = -w_e * gamma_l, RX theta = 2 * beta_l)."""
+        p = len(self.gammas)
+        gates = self.circuit()
+        binding = np.zeros(len(gates), dtype=PARAM_DTYPE)
+        binding["idx"] = -1
+        k = self.n
+        for layer in range(p):
+            for w in self.weights:
+                binding[k]["idx"][0] = layer
+                binding[k]["coef"][0] = -float(w)
+                k += 1
+            for _ in range(self.n):
+                binding[k]["idx"][0] = p + layer
+                binding[k]["coef"][0] = 2.0
+                k += 1
+        params = np.concatenate([self.gammas, self.betas]).astype(np.float64)
+        return ParamCircuit(self.n, gates, binding, params)
+
+    def maxcut_terms(self) -> np.ndarray:
+        """C = sum_e w_e (1 - Z_a Z_b) / 2 as Pauli terms."""
+        terms = np.zeros(len(self.edges) + 1, dtype=PAULI_DTYPE)
+        terms[0] = (0.5 * float(np.sum(self.weights)), 0, 0)
+        for k, ((a, b), w) in enumerate(zip(self.edges, self.weights)):
+            terms[k + 1] = (-0.5 * float(w), 0, (1 << int(a)) | (1 << int(b)))
+        return terms
+
 
 def qaoa_instances(count: int = 512, n_min: int = 10, n_max: int = 22, p: int = 4,
                    edge_prob: float = 0.3, seed: int = 99) -> list[QaoaInstance]:

@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import numpy as np
+
 import pytest
 
 from conftest import HAS_GPU, ROOT
@@ -76,3 +78,28 @@ def test_reference_binding_module_imports():
         assert hasattr(libsvsim.Simulation, name)
     for meth in ("append", "upload", "run", "measure", "reset", "clear_circuit"):
         assert hasattr(libsvsim.Simulation, meth)
+
+
+def test_qaoa_batch_arguments_rejected_without_touching_the_gpu(lib):
+    from svsim_b200 import _native
+    L = _native.lib()
+    b = ctypes.c_void_p()
+    nq = np.array([4, 25], dtype=np.uint32)            # 25 > 2 * 12 tile bits (FP64)
+    eoff = np.array([0, 1, 2], dtype=np.uint32)
+    edges = np.array([0, 1, 0, 1], dtype=np.uint32)
+    w = np.ones(2)
+    args = (nq.ctypes.data, eoff.ctypes.data, edges.ctypes.data, w.ctypes.data)
+    assert L.svb_qaoa_create(0, 0, 2, *args, 2, ctypes.byref(b)) == _native.SVB_ERR_INVALID
+    assert b"instance 1" in L.svb_last_error()
+    nq[1] = 5
+    edges[3] = 7                                        # qubit 7 outside [0, 5)
+    assert L.svb_qaoa_create(0, 0, 2, *args, 2, ctypes.byref(b)) == _native.SVB_ERR_INVALID
+    assert b"edge" in L.svb_last_error()
+    edges[3] = 0                                        # a loop
+    assert L.svb_qaoa_create(0, 0, 2, *args, 2, ctypes.byref(b)) == _native.SVB_ERR_INVALID
+    edges[3] = 1
+    assert L.svb_qaoa_create(0, 0, 2, *args, 0, ctypes.byref(b)) == _native.SVB_ERR_INVALID
+    assert L.svb_qaoa_create(0, 5, 2, *args, 2, ctypes.byref(b)) == _native.SVB_ERR_INVALID
+    assert not b.value
+    assert L.svb_qaoa_run(None, None, None, None, None) == _native.SVB_ERR_INVALID
+    assert L.svb_qaoa_destroy(None) == _native.SVB_OK
