@@ -52,6 +52,12 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS,
                     help="state size (smaller cases are for profiling only)")
     ap.add_argument("--tile-bits", type=int, default=12)
+    ap.add_argument("--form", choices=["headline", "fused", "qaoa", "capacity"], default="headline",
+                    help="headline: the FP64 n=30 step (the measured line); the others run one "
+                         "secondary form alone (for profiling and capacity runs)")
+    ap.add_argument("--instances", type=int, default=512, help="QAOA batch size (--form qaoa)")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
+                    help="state precision of --form qaoa")
     return ap.parse_args()
 
 
@@ -312,16 +318,16 @@ def run_ours(args):
         print(json.dumps(out))
 
 
-def fused_form(device, circuit, k=5, reps=3):
+def fused_form(device, circuit, k=5, reps=3, n=N_QUBITS):
     """The same circuit on an FP32 state through the fused tensor-core engine, with its
     fidelity and largest amplitude error against the FP64 staged result."""
     import torch
     from svsim_b200 import _native as nat
-    h64 = nat.Handle(N_QUBITS, device, nat.SVB_FP64)
-    h64.set_engine(nat.ENGINE_STAGED, 12, 0)
+    h64 = nat.Handle(n, device, nat.SVB_FP64)
+    h64.set_engine(nat.ENGINE_STAGED, 12 if n >= 20 else 0, 0)
     h64.set_circuit(circuit)
     h64.run()
-    h32 = nat.Handle(N_QUBITS, device, nat.SVB_FP32)
+    h32 = nat.Handle(n, device, nat.SVB_FP32)
     h32.set_engine(nat.ENGINE_FUSED, 0, k)
     h32.set_circuit(circuit)
     info = h32.plan_info()
@@ -351,6 +357,101 @@ def fused_form(device, circuit, k=5, reps=3):
     return out
 
 
+def qaoa_form(device, count=512, precision="fp64", reps=5):
+    """Batched QAOA: energy and gradient of every instance per evaluation; kernel timed
+    alone on the device (parameters resident) and end to end through svb_qaoa_run (host
+    parameters in, host energies and gradients out)."""
+    import torch
+    from svsim_b200 import circuits, _native as nat
+    insts = circuits.qaoa_instances(count)
+    g = np.stack([i.gammas for i in insts])
+    b = np.stack([i.betas for i in insts])
+    prec = nat.SVB_FP64 if precision == "fp64" else nat.SVB_FP32
+    B = nat.QaoaBatch(insts, device, prec)
+    st = B.info()
+    B.run(g, b)
+    s = torch.cuda.Stream(device)
+    for _ in range(3):
+        B.launch(s.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    e0.record(s)
+    for _ in range(reps):
+        B.launch(s.cuda_stream)
+    e1.record(s)
+    torch.cuda.synchronize(device)
+    sec = e0.elapsed_time(e1) / 1e3 / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        B.run(g, b)
+    e2e = (time.perf_counter() - t0) / reps
+    B.close()
+    torch.cuda.empty_cache()
+    peak, kind = peaks()
+    return {"instances_per_s": count / sec, "ms_per_batch": sec * 1e3,
+            "e2e_instances_per_s": count / e2e, "e2e_ms_per_batch": e2e * 1e3,
+            "hbm_gbs": st.moved_bytes / sec / 1e9, "frac_of_peak": st.moved_bytes / sec / 1e9 / peak,
+            "moved_bytes_per_batch": st.moved_bytes, "total_amplitudes": int(st.total_amplitudes),
+            "tiles_per_pass": int(st.tiles_per_pass), "graphed": bool(st.graphed),
+            "precision": precision, "p": int(st.p), "grid": int(st.grid),
+            "e2e_h2d_bytes": int(g.nbytes + b.nbytes), "e2e_d2h_bytes": int(count * (1 + 2 * st.p) * 8 + 4),
+            "kernel": "k_qaoa (one cooperative launch: 4p tile passes, grid barriers between)",
+            "workload": f"{count} MaxCut instances, n ~ U{{10..22}}, G(n,0.3), p=4"}
+
+
+def capacity_form(device, shots=4096):
+    """The largest states of one B200: n=33 FP64 (staged, 128 GiB) and n=34 FP32 (fused,
+    128 GiB), depth-20 random-matching circuits, 4096-shot sampling with the FP64 CDF."""
+    import torch
+    from svsim_b200 import circuits, _native as nat
+    out = {}
+    uni = np.random.default_rng(1).random(shots)
+    for n, prec, eng, k, name in ((33, nat.SVB_FP64, nat.ENGINE_STAGED, 0, "n33_fp64_staged"),
+                                  (34, nat.SVB_FP32, nat.ENGINE_FUSED, 5, "n34_fp32_fused")):
+        circ = circuits.random_matching_circuit(n, 20, seed=SEED)
+        h = nat.Handle(n, device, prec)
+        h.set_engine(eng, 0, k)
+        h.set_circuit(circ)
+        info = h.plan_info()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        h.run()
+        e1.record()
+        torch.cuda.synchronize(device)
+        h.sync()
+        sec = e0.elapsed_time(e1) / 1e3
+        t0 = time.perf_counter()
+        samples, total = h.measure(uni)
+        t_meas = time.perf_counter() - t0
+        out[name] = {"gates_per_s": len(circ) / sec, "s_per_circuit": sec, "passes": int(info.n_passes),
+                     "state_gib": info.state_bytes / 2**30, "hbm_gbs": info.moved_bytes / sec / 1e9,
+                     "shots": shots, "measure_s": t_meas, "prob_total": total,
+                     "distinct_outcomes": int(len(np.unique(samples)))}
+        del h
+        torch.cuda.empty_cache()
+    return out
+
+
+def run_form(args):
+    """One secondary form alone, as one JSON line (rank 0 only)."""
+    import torch
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    if args.form == "fused":
+        circuit = None
+        from svsim_b200 import circuits
+        circuit = circuits.random_matching_circuit(args.qubits, DEPTH, seed=SEED)
+        res = fused_form(local, circuit, n=args.qubits, reps=max(1, args.steps))
+    elif args.form == "qaoa":
+        res = qaoa_form(local, args.instances, args.precision, reps=max(1, args.steps))
+    else:
+        res = capacity_form(local)
+    print(json.dumps({"form": args.form, **res}))
+
+
 def secondary_forms(device, circuit):
     """Per-gate FP64 sweeps on the same circuit, and adjoint gradients (n=20, 480 params)."""
     import torch
@@ -377,6 +478,9 @@ def secondary_forms(device, circuit):
     del h
     torch.cuda.empty_cache()
     forms["fused_tc_fp32"] = fused_form(device, circuit)
+    forms["qaoa_batch_fp64"] = qaoa_form(device, 512, "fp64")
+    forms["qaoa_batch_fp32"] = qaoa_form(device, 512, "fp32")
+    forms["capacity"] = capacity_form(device)
     # adjoint: n=20 hardware-efficient ansatz, 720 gates, 480 parameters
     pc = circuits.hardware_efficient_ansatz()
     terms = circuits.zz_x_hamiltonian(20)
@@ -412,6 +516,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.form != "headline":
+        run_form(args)
     else:
         run_ours(args)
 

@@ -192,10 +192,11 @@ __device__ __forceinline__ void rx_pair(V& a0, V& a1, T c, T s)
     a1.y = +(s * a0r) + (c * a1i);
 }
 
+// Im(conj(l) p), in the state's precision (sums are widened to FP64 once per stage)
 template <typename V>
-__device__ __forceinline__ double im_conj_mul(const V& l, const V& p)
+__device__ __forceinline__ auto im_conj_mul(const V& l, const V& p) -> decltype(l.x)
 {
-    return (double)l.x * (double)p.y - (double)l.y * (double)p.x;
+    return l.x * p.y - l.y * p.x;
 }
 
 // RX on every owned register slot of stage S whose local bit lies in [jb, je).  On the
@@ -206,6 +207,7 @@ __device__ __forceinline__ void stage_rx(typename AmpOf<T>::type* ps, typename A
                                          int jb, int je, T c, T s, double& part_b)
 {
     using C = QbCfg<T>;
+    T acc = T(0);
 #pragma unroll
     for (int j = 0; j < C::RB; j++) {
         if (!C::owns(S, j)) continue;
@@ -216,7 +218,7 @@ __device__ __forceinline__ void stage_rx(typename AmpOf<T>::type* ps, typename A
             if (k & (1 << j)) continue;
             const int k1 = k | (1 << j);
             if (REV) {
-                part_b += im_conj_mul(ls[k], ps[k1]) + im_conj_mul(ls[k1], ps[k]);
+                acc += im_conj_mul(ls[k], ps[k1]) + im_conj_mul(ls[k1], ps[k]);
                 rx_pair(ps[k], ps[k1], c, T(-s));
                 rx_pair(ls[k], ls[k1], c, T(-s));
             } else {
@@ -224,6 +226,7 @@ __device__ __forceinline__ void stage_rx(typename AmpOf<T>::type* ps, typename A
             }
         }
     }
+    if (REV) part_b += static_cast<double>(acc);
 }
 
 template <typename T, int SF, int ST>
@@ -238,15 +241,8 @@ __device__ __forceinline__ void exchange(typename AmpOf<T>::type* r, typename Am
     for (int k = 0; k < C::NR; k++) r[k] = buf[swz<T>(tb_to | reg_off<T, ST>(k))];
 }
 
-template <typename T>
-__device__ __forceinline__ void cis(double ang, T& cr, T& ci);
-template <>
-__device__ __forceinline__ void cis<double>(double ang, double& cr, double& ci) { sincos(ang, &ci, &cr); }
-template <>
-__device__ __forceinline__ void cis<float>(double ang, float& cr, float& ci)
-{
-    sincosf(static_cast<float>(ang), &ci, &cr);
-}
+__device__ __forceinline__ void cis(double ang, double& cr, double& ci) { sincos(ang, &ci, &cr); }
+__device__ __forceinline__ void cis(float ang, float& cr, float& ci) { sincosf(ang, &ci, &cr); }
 
 template <typename V, typename T>
 __device__ __forceinline__ V cmul(const V& a, T cr, T ci)
@@ -304,6 +300,7 @@ __global__ void __launch_bounds__(QB_THREADS, 1) k_qaoa(QaoaArgs A)
             const bool last_fwd = fwd && layer == P - 1 && (high || n <= M);
             const double gamma = A.gammas[lo * P + layer], beta = A.betas[lo * P + layer];
             const T c = static_cast<T>(cos(beta)), s = static_cast<T>(-sin(beta));
+            const T gam = static_cast<T>(gamma);
             V* gp = psi + D.state_off;
             V* gl = lam + D.state_off;
             const T* gc = cost + D.state_off;
@@ -336,9 +333,9 @@ __global__ void __launch_bounds__(QB_THREADS, 1) k_qaoa(QaoaArgs A)
 #pragma unroll
                 for (int k = 0; k < NR; k++) {
                     const uint32_t l = tb0 | reg_off<T, 0>(k);
-                    const double cz = l < size ? (double)gc[tm.z(l)] : 0.0;
+                    const T cz = l < size ? gc[tm.z(l)] : T(0);
                     T cr, ci;
-                    cis<T>(-gamma * cz, cr, ci);
+                    cis(-gam * cz, cr, ci);
                     ps[k] = cmul(ps[k], cr, ci);
                 }
             }
@@ -369,27 +366,31 @@ __global__ void __launch_bounds__(QB_THREADS, 1) k_qaoa(QaoaArgs A)
             }
             // stage 3: diagonal work on the final layout, then registers -> HBM
             if (last_fwd) {
+                T acc = T(0);
 #pragma unroll
                 for (int k = 0; k < NR; k++) {
                     const uint32_t l = tb3 | reg_off<T, 3>(k);
-                    const double cz = l < size ? (double)gc[tm.z(l)] : 0.0;
-                    const double pr = ps[k].x, pi = ps[k].y;
-                    part_e += cz * (pr * pr + pi * pi);
-                    ls[k].x = static_cast<T>(cz * pr);
-                    ls[k].y = static_cast<T>(cz * pi);
+                    const T cz = l < size ? gc[tm.z(l)] : T(0);
+                    const T pr = ps[k].x, pi = ps[k].y;
+                    acc += cz * (pr * pr + pi * pi);
+                    ls[k].x = cz * pr;
+                    ls[k].y = cz * pi;
                 }
+                part_e = static_cast<double>(acc);
             }
             if (!fwd && !high) {
+                T acc = T(0);
 #pragma unroll
                 for (int k = 0; k < NR; k++) {
                     const uint32_t l = tb3 | reg_off<T, 3>(k);
-                    const double cz = l < size ? (double)gc[tm.z(l)] : 0.0;
-                    part_g += cz * im_conj_mul(ls[k], ps[k]);
+                    const T cz = l < size ? gc[tm.z(l)] : T(0);
+                    acc += cz * im_conj_mul(ls[k], ps[k]);
                     T cr, ci;
-                    cis<T>(gamma * cz, cr, ci);
+                    cis(gam * cz, cr, ci);
                     ps[k] = cmul(ps[k], cr, ci);
                     ls[k] = cmul(ls[k], cr, ci);
                 }
+                part_g = static_cast<double>(acc);
             }
             const bool store_psi = fwd || layer > 0 || high;
             const bool store_lam = (!fwd && store_psi) || last_fwd;

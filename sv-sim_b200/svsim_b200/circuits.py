@@ -59,6 +59,21 @@ def random_matching_circuit(n: int = 30, depth: int = 40, seed: int = 2024) -> n
     return _pack(rows)
 
 
+def inverse_circuit(gates: np.ndarray) -> np.ndarray:
+    """The inverse gate list of a U3/CX/H/X circuit: reversed order, U3(t, p, l) ->
+    U3(-t, -l, -p) (the conjugate transpose of the reference's U3 matrix), CX, H, X
+    self-inverse."""
+    out = np.ascontiguousarray(gates[::-1].copy())
+    for g in out:
+        op = int(g["op"])
+        if op == OP["U3"]:
+            t, p, l = float(g["theta"]), float(g["phi"]), float(g["lam"])
+            g["theta"], g["phi"], g["lam"] = -t, -l, -p
+        elif op not in (OP["CX"], OP["H"], OP["X"]):
+            raise ValueError(f"inverse_circuit: op {op} not supported")
+    return out
+
+
 @dataclass
 class ParamCircuit:
     """A circuit whose angles depend affinely on a parameter vector:
