@@ -334,6 +334,7 @@ def fused_form(device, circuit, k=5, reps=3, n=N_QUBITS):
     h32.run()
     h32.sync()
     fid, maxd = h64.compare(h32)
+    norm32 = h32.norm2()
     del h64
     torch.cuda.empty_cache()
     h32.run()
@@ -351,6 +352,7 @@ def fused_form(device, circuit, k=5, reps=3, n=N_QUBITS):
            "passes": int(info.n_passes), "hbm_gbs": info.moved_bytes / s / 1e9,
            "hbm_frac_of_peak": info.moved_bytes / s / 1e9 / peak,
            "one_minus_fidelity_vs_fp64": 1.0 - fid, "max_abs_amp_err_vs_fp64": maxd,
+           "norm_minus_one": norm32 - 1.0,
            "kernel": "k_fused<5>: split-TF32 tcgen05.mma (M=128, N=K=64), TMEM accumulators"}
     del h32
     torch.cuda.empty_cache()

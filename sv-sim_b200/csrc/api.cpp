@@ -69,6 +69,7 @@ void free_plan(Sim* s)
     cudaFree(s->dfused.blocks);
     cudaFree(s->dfused.gates);
     cudaFree(s->dfused.err);
+    cudaFree(s->dfused.norm_partial);
     s->dfused = DevFusedBuffers{};
     s->fused = FusedPlan{};
     s->eops.clear();
@@ -146,6 +147,10 @@ svb_status launch_all(Sim* s, cudaStream_t st)
             cudaError_t e = launch_fused_pass(s->state, n, F.k, (int)p, F.passes[p].n_blocks, 0,
                                               s->dfused, st);
             if (e != cudaSuccess) return cuda_fail(e, "fused pass launch");
+        }
+        if (!F.passes.empty()) {
+            cudaError_t e = launch_fused_renorm(s->state, n, s->dfused, st);
+            if (e != cudaSuccess) return cuda_fail(e, "fused renormalisation");
         }
         return SVB_OK;
     }
@@ -376,6 +381,7 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
                  "cudaMalloc(plan)");
         SVB_CUDA(cudaMalloc(&s->dfused.err, sizeof(int)), "cudaMalloc(flag)");
         SVB_CUDA(cudaMemset(s->dfused.err, 0, sizeof(int)), "cudaMemset");
+        SVB_CUDA(cudaMalloc(&s->dfused.norm_partial, REDUCE_BLOCKS * sizeof(double)), "cudaMalloc(norm)");
         if (!F.passes.empty())
             SVB_CUDA(cudaMemcpy(s->dfused.passes, F.passes.data(), F.passes.size() * sizeof(FusedPass),
                                 cudaMemcpyHostToDevice), "plan upload");
@@ -389,7 +395,8 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
         s->info.tile_bits = FT_TILE_BITS;
         s->info.plan_bytes = F.passes.size() * sizeof(FusedPass) + F.blocks.size() * sizeof(FusedBlock) +
                              F.gates.size() * sizeof(float);
-        s->info.moved_bytes = 2.0 * sb * (double)F.passes.size();
+        // one read + write per pass, then the renormalisation (two reads, one write)
+        s->info.moved_bytes = 2.0 * sb * (double)F.passes.size() + (F.passes.empty() ? 0.0 : 3.0 * sb);
     } else if (engine == SVB_ENGINE_STAGED) {
         const int G = s->precision == SVB_FP64 ? 3 : 4;
         plan_staged(s->eops, n, M, G, s->staged);

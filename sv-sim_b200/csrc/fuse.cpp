@@ -284,11 +284,12 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
                     double val;
                     if (cr == 0) val = cc == 0 ? u.real() : -u.imag();
                     else val = cc == 0 ? u.imag() : u.real();
-                    const float fv = (float)val;
-                    const float h = tf32_hi(fv);
+                    // hi = val to TF32, lo = the remainder to TF32 (both rounded to
+                    // nearest, so the pair carries ~21 bits of the FP64 entry, unbiased)
+                    const float h = tf32_hi((float)val);
                     const uint32_t w = kmajor_offset(mp, kk, N) / 4;
                     hi[w] = h;
-                    lo[w] = fv - h;
+                    lo[w] = tf32_hi((float)(val - (double)h));
                 }
             }
             plan.blocks.push_back(B);

@@ -10,7 +10,7 @@
 //        D[n][m'] = sum_kk X[n][kk] G[m'][kk]
 // with tcgen05.mma.kind::tf32 (M = 128 rows per MMA, N = 2^(k+1), K = 8 per
 // instruction) accumulating in TMEM, in three products X_hi G_hi + X_hi G_lo + X_lo G_hi
-// (split TF32: hi = x rounded to TF32, lo = x - hi), so the result keeps ~FP32
+// (split TF32: hi = x rounded to TF32, lo = x - hi rounded to TF32), so the result keeps ~FP32
 // accuracy.  Both operands sit in shared memory in the canonical K-major, no-swizzle
 // layout (8-row x 16-byte core matrices).  Each thread then reads its D row (one row n,
 // all 2^k amplitudes) with tcgen05.ld and scatters it, split again into hi/lo, into the
@@ -135,12 +135,15 @@ struct FusedSmem {
 };
 
 // Writes amplitude (re, im) at word offset w of the state operand (re and im are adjacent
-// K values, 8-byte aligned), split into the TF32 hi plane and the FP32 remainder plane.
+// K values, 8-byte aligned), split into a TF32 hi plane and a TF32 lo plane.  Both
+// parts are rounded to nearest explicitly: the MMA reads only the upper 19 bits of each
+// FP32 word, and a remainder left in full FP32 would lose its low bits by truncation,
+// i.e. always towards zero, which shrinks the norm a little at every block.
 __device__ __forceinline__ void put_operand(float* xh, float* xl, uint32_t w, float re, float im)
 {
     const float hr = tf32_rna(re), hi = tf32_rna(im);
     *reinterpret_cast<float2*>(xh + w) = make_float2(hr, hi);
-    *reinterpret_cast<float2*>(xl + w) = make_float2(re - hr, im - hi);
+    *reinterpret_cast<float2*>(xl + w) = make_float2(tf32_rna(re - hr), tf32_rna(im - hi));
 }
 
 template <int K>
@@ -363,7 +366,67 @@ cudaError_t launch_k(void* state, int n, int pass_index, const DevFusedBuffers& 
     return cudaGetLastError();
 }
 
+// FP64 sum of |a|^2 per block (grid-stride, fixed order within a block)
+__global__ void __launch_bounds__(256) k_norm_partial(const float4* __restrict__ sv, uint64_t pairs,
+                                                      double* __restrict__ partial)
+{
+    __shared__ double red[8];
+    double acc = 0.0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < pairs;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float4 v = sv[i];
+        acc += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < 8; w++) s += red[w];
+        partial[blockIdx.x] = s;
+    }
+}
+
+// a <- a / sqrt(sum |a|^2); every block forms the same total from the partials in the
+// same order, so the scale is identical everywhere
+__global__ void __launch_bounds__(256) k_renorm(float4* __restrict__ sv, uint64_t pairs,
+                                                const double* __restrict__ partial, int np)
+{
+    __shared__ float scale;
+    if (threadIdx.x < 32) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < np; i += 32) s += partial[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) scale = s > 0.0 ? (float)(1.0 / sqrt(s)) : 1.0f;
+    }
+    __syncthreads();
+    const float f = scale;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < pairs;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        float4 v = sv[i];
+        v.x *= f; v.y *= f; v.z *= f; v.w *= f;
+        sv[i] = v;
+    }
+}
+
 }  // namespace
+
+// The tensor cores accumulate the FP32 sums of an MMA with truncation (round towards
+// zero), so every fused block takes a fraction of an ulp off each amplitude's magnitude
+// and the norm of an FP32 fused run decays slowly (about 1e-7 per gate).  The decay is
+// nearly uniform over the amplitudes, so one FP64 renormalisation after the run removes
+// it: two reads and one write of the state.
+cudaError_t launch_fused_renorm(void* state, int n, const DevFusedBuffers& b, cudaStream_t s)
+{
+    if (n < FT_TILE_BITS || !b.norm_partial) return cudaErrorInvalidValue;
+    const uint64_t pairs = 1ull << (n - 1);
+    float4* sv = static_cast<float4*>(state);
+    k_norm_partial<<<REDUCE_BLOCKS, 256, 0, s>>>(sv, pairs, b.norm_partial);
+    k_renorm<<<REDUCE_BLOCKS * 2, 256, 0, s>>>(sv, pairs, b.norm_partial, REDUCE_BLOCKS);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_fused_pass(void* state, int n, int k, int pass_index, int n_blocks,
                               int gate_words_per_block, const DevFusedBuffers& b, cudaStream_t s)

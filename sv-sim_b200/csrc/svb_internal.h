@@ -174,9 +174,12 @@ struct DevFusedBuffers {
     FusedBlock* blocks = nullptr;
     float* gates = nullptr;
     int* err = nullptr;
+    double* norm_partial = nullptr;      // REDUCE_BLOCKS FP64 partial sums of |a|^2
 };
 cudaError_t launch_fused_pass(void* state, int n, int k, int pass_index, int n_blocks,
                               int gate_words_per_block, const DevFusedBuffers& b, cudaStream_t s);
+// Rescales the FP32 state to unit norm (norm summed in FP64) after a fused run.
+cudaError_t launch_fused_renorm(void* state, int n, const DevFusedBuffers& b, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------
 // Kernel launchers (kernels_apply.cu)

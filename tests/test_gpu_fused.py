@@ -73,3 +73,20 @@ def test_fused_rejects_srn_and_fp64():
     h64 = nat.Handle(12, 0, nat.SVB_FP64)
     with pytest.raises(nat.SvbError):
         h64.set_engine(nat.ENGINE_FUSED, 0, 4)
+
+
+def test_fused_run_keeps_unit_norm_and_small_amplitude_error():
+    """The tensor cores truncate their FP32 sums, so without the closing FP64
+    renormalisation the norm of a deep fused run decays by ~1e-7 per gate; with it the
+    norm stays 1 to FP32 rounding and the largest amplitude error stays at FP32 level."""
+    from svsim_b200 import _native as nat
+    n = 20
+    g = circuits.random_matching_circuit(n, 40, seed=9)
+    h32 = run_fused(n, g, 5)
+    assert abs(h32.norm2() - 1.0) <= 2e-6
+    h64 = nat.Handle(n, 0, nat.SVB_FP64)
+    h64.set_circuit(g)
+    h64.run()
+    f, d = h64.compare(h32)
+    amp = 2.0 ** (-n / 2)
+    assert 1 - f <= 1e-9 and d <= 2e-4 * amp, (1 - f, d)
