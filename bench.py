@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS,
                     help="state size (smaller cases are for profiling only)")
     ap.add_argument("--tile-bits", type=int, default=12)
-    ap.add_argument("--form", choices=["headline", "fused", "qaoa", "capacity"], default="headline",
+    ap.add_argument("--form", choices=["headline", "pergate", "fused", "qaoa", "capacity"], default="headline",
                     help="headline: the FP64 n=30 step (the measured line); the others run one "
                          "secondary form alone (for profiling and capacity runs)")
     ap.add_argument("--instances", type=int, default=512, help="QAOA batch size (--form qaoa)")
@@ -435,14 +435,60 @@ def capacity_form(device, shots=4096):
     return out
 
 
+def qaoa_sharded_form(args, world, rank, local):
+    """Batched QAOA split over the ranks (one GPU each, size-balanced, results gathered by
+    one all-reduce).  Each step is one full evaluation through ShardedQaoa.run with host
+    parameters in and host results out; the time is the max over ranks."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from svsim_b200 import circuits, _native as nat
+    from svsim_b200.sharding import ShardedQaoa
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    insts = circuits.qaoa_instances(args.instances)
+    g = np.stack([i.gammas for i in insts])
+    b = np.stack([i.betas for i in insts])
+    prec = nat.SVB_FP64 if args.precision == "fp64" else nat.SVB_FP32
+    sq = ShardedQaoa(insts, device=local, precision=prec)
+    for _ in range(max(args.warmup, 3)):
+        sq.run(g, b)
+    dist.barrier()
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sq.run(g, b)
+    torch.cuda.synchronize(local)
+    dt = time.perf_counter() - t0
+    t = torch.tensor([dt], device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dt = float(t.item())
+    mine_amps = sum(1 << insts[i].n for i in sq.mine)
+    sq.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    return {"form": "qaoa", "instances_per_s": args.instances * args.steps / dt,
+            "ms_per_batch": dt / args.steps * 1e3, "n_gpus": world, "precision": args.precision,
+            "scaling": "strong", "rank0_instances": len(sq.mine), "rank0_amplitudes": mine_amps,
+            "path": "ShardedQaoa.run: host parameters in, per-rank svb_qaoa_run, all-reduce gather"}
+
+
 def run_form(args):
-    """One secondary form alone, as one JSON line (rank 0 only)."""
+    """One secondary form alone, as one JSON line (rank 0 prints)."""
     import torch
     world, rank, local = dist_env()
+    if args.form == "qaoa" and world > 1:
+        res = qaoa_sharded_form(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(res))
+        return
     if rank != 0:
         return
     torch.cuda.set_device(local)
-    if args.form == "fused":
+    if args.form == "pergate":
+        from svsim_b200 import circuits
+        res = per_gate_form(local, circuits.random_matching_circuit(args.qubits, DEPTH, seed=SEED), n=args.qubits)
+    elif args.form == "fused":
         circuit = None
         from svsim_b200 import circuits
         circuit = circuits.random_matching_circuit(args.qubits, DEPTH, seed=SEED)
@@ -454,13 +500,12 @@ def run_form(args):
     print(json.dumps({"form": args.form, **res}))
 
 
-def secondary_forms(device, circuit):
-    """Per-gate FP64 sweeps on the same circuit, and adjoint gradients (n=20, 480 params)."""
+def per_gate_form(device, circuit, n=N_QUBITS):
+    """The per-gate FP64 engine (one HBM sweep per elementary op, as the reference) on
+    the first 4 layers (180 gates) of the circuit."""
     import torch
-    from svsim_b200 import circuits, _native as nat
-    forms = {}
-    # per-gate engine on the first 4 layers (180 gates): one kernel per elementary op
-    h = nat.Handle(N_QUBITS, device, nat.SVB_FP64)
+    from svsim_b200 import _native as nat
+    h = nat.Handle(n, device, nat.SVB_FP64)
     h.set_engine(nat.ENGINE_PER_GATE, 0, 0)
     sub = circuit[:180]
     h.set_circuit(sub)
@@ -474,11 +519,20 @@ def secondary_forms(device, circuit):
     torch.cuda.synchronize(device)
     s = e0.elapsed_time(e1) / 1e3
     peak, _ = peaks()
-    forms["per_gate_fp64"] = {"gates_per_s": len(sub) / s, "hbm_gbs": info.moved_bytes / s / 1e9,
-                              "frac_of_peak": info.moved_bytes / s / 1e9 / peak,
-                              "sample": "first 4 layers (180 gates), one sweep per gate"}
     del h
     torch.cuda.empty_cache()
+    return {"gates_per_s": len(sub) / s, "hbm_gbs": info.moved_bytes / s / 1e9,
+            "frac_of_peak": info.moved_bytes / s / 1e9 / peak,
+            "sample": "first 4 layers (180 gates), one sweep per gate (CX: half sweep)",
+            "kernels": "k_eop_pairs / k_cx (4 pairs per thread in flight)"}
+
+
+def secondary_forms(device, circuit):
+    """Per-gate FP64 sweeps on the same circuit, and adjoint gradients (n=20, 480 params)."""
+    import torch
+    from svsim_b200 import circuits, _native as nat
+    forms = {}
+    forms["per_gate_fp64"] = per_gate_form(device, circuit)
     forms["fused_tc_fp32"] = fused_form(device, circuit)
     forms["qaoa_batch_fp64"] = qaoa_form(device, 512, "fp64")
     forms["qaoa_batch_fp32"] = qaoa_form(device, 512, "fp32")

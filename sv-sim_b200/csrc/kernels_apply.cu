@@ -19,6 +19,11 @@ namespace svb {
 // ---------------------------------------------------------------------------------
 // per-gate engine
 // ---------------------------------------------------------------------------------
+// Each thread takes PG_UNROLL items per iteration (items u * stride apart, so a warp's
+// accesses stay coalesced) and issues all their loads before any arithmetic: more bytes
+// in flight per thread than one pair at a time.
+constexpr int PG_UNROLL = 4;
+
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_eop_pairs(typename VecOf<T>::type* __restrict__ sv, uint64_t half, int q, int form,
@@ -28,23 +33,31 @@ k_eop_pairs(typename VecOf<T>::type* __restrict__ sv, uint64_t half, int q, int 
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t qd = 1ull << q;
     const bool diag = form_is_diag(form);
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < half; i += stride) {
-        const uint64_t p0 = insert_zero(i, q);
-        const uint64_t p1 = p0 | qd;
-        if (diag) {
-            V a1 = sv[p1];
-            diag_one<T>(form, c, a1);
-            sv[p1] = a1;
-            if (form == F_DIAG) {
-                V a0 = sv[p0];
-                diag_zero<T>(form, c, a0);
-                sv[p0] = a0;
+    const bool both = !diag || form == F_DIAG;     // diagonal forms other than D leave |0> alone
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < half;
+         i0 += PG_UNROLL * stride) {
+        V a0[PG_UNROLL], a1[PG_UNROLL];
+        uint64_t p0[PG_UNROLL];
+#pragma unroll
+        for (int u = 0; u < PG_UNROLL; u++) {
+            const uint64_t i = i0 + (uint64_t)u * stride;
+            p0[u] = insert_zero(i < half ? i : 0, q);
+            if (i < half) {
+                a1[u] = sv[p0[u] | qd];
+                if (both) a0[u] = sv[p0[u]];
             }
-        } else {
-            V a0 = sv[p0], a1 = sv[p1];
-            dense_pair<T>(form, c, a0, a1);
-            sv[p0] = a0;
-            sv[p1] = a1;
+        }
+#pragma unroll
+        for (int u = 0; u < PG_UNROLL; u++) {
+            if (i0 + (uint64_t)u * stride >= half) continue;
+            if (diag) {
+                diag_one<T>(form, c, a1[u]);
+                if (form == F_DIAG) diag_zero<T>(form, c, a0[u]);
+            } else {
+                dense_pair<T>(form, c, a0[u], a1[u]);
+            }
+            sv[p0[u] | qd] = a1[u];
+            if (both) sv[p0[u]] = a0[u];
         }
     }
 }
@@ -58,21 +71,33 @@ k_cx(typename VecOf<T>::type* __restrict__ sv, uint64_t quarter, int c, int t)
     const int lo = c < t ? c : t, hi = c < t ? t : c;
     const uint64_t cd = 1ull << c, td = 1ull << t;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < quarter; i += stride) {
-        const uint64_t b = insert_zero(insert_zero(i, lo), hi);
-        const uint64_t p0 = b | cd, p1 = b | cd | td;
-        const V a0 = sv[p0];
-        const V a1 = sv[p1];
-        sv[p0] = a1;
-        sv[p1] = a0;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < quarter;
+         i0 += PG_UNROLL * stride) {
+        V a0[PG_UNROLL], a1[PG_UNROLL];
+        uint64_t b[PG_UNROLL];
+#pragma unroll
+        for (int u = 0; u < PG_UNROLL; u++) {
+            const uint64_t i = i0 + (uint64_t)u * stride;
+            b[u] = insert_zero(insert_zero(i < quarter ? i : 0, lo), hi) | cd;
+            if (i < quarter) {
+                a0[u] = sv[b[u]];
+                a1[u] = sv[b[u] | td];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < PG_UNROLL; u++) {
+            if (i0 + (uint64_t)u * stride >= quarter) continue;
+            sv[b[u]] = a1[u];
+            sv[b[u] | td] = a0[u];
+        }
     }
 }
 
 static unsigned grid_for(uint64_t items, int threads)
 {
     // enough CTAs to fill 148 SMs several times over, grid-stride beyond that
-    const uint64_t need = (items + threads - 1) / threads;
-    const uint64_t cap = 148ull * 16;
+    const uint64_t need = (items + (uint64_t)threads * PG_UNROLL - 1) / ((uint64_t)threads * PG_UNROLL);
+    const uint64_t cap = 148ull * 8;
     return (unsigned)(need < cap ? (need > 0 ? need : 1) : cap);
 }
 

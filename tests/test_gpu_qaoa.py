@@ -140,3 +140,16 @@ def test_headline_batch_512_instances():
     b.close()
     e32, g32 = nat.QaoaBatch(insts, 0, nat.SVB_FP32).run(g, bt)
     assert np.max(np.abs(e32 - e) / np.maximum(1.0, np.abs(e))) <= 1e-4
+
+
+def test_sharded_wrapper_single_process_equals_batch():
+    """ShardedQaoa without torch.distributed is the plain batch on one GPU."""
+    from svsim_b200 import _native as nat
+    from svsim_b200.sharding import ShardedQaoa
+    insts = circuits.qaoa_instances(24, n_min=6, n_max=16, seed=4)
+    g, bt = params_of(insts)
+    e0, g0 = nat.QaoaBatch(insts, 0, nat.SVB_FP64).run(g, bt)
+    sq = ShardedQaoa(insts, device=0, precision=nat.SVB_FP64)
+    e1, g1 = sq.run(g, bt)
+    sq.close()
+    assert np.array_equal(e0, e1) and np.array_equal(g0, g1)
