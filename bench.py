@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS,
                     help="state size (smaller cases are for profiling only)")
     ap.add_argument("--tile-bits", type=int, default=12)
+    ap.add_argument("--engine", choices=["staged", "pairs"], default="pairs",
+                    help="FP64 engine of the headline step")
     ap.add_argument("--form", choices=["headline", "pergate", "fused", "qaoa", "capacity"], default="headline",
                     help="headline: the FP64 n=30 step (the measured line); the others run one "
                          "secondary form alone (for profiling and capacity runs)")
@@ -213,7 +215,10 @@ def run_ours(args):
     n_gates = len(circuit)
 
     h = nat.Handle(nq, device, nat.SVB_FP64)
-    h.set_engine(nat.ENGINE_STAGED, args.tile_bits, 0)
+    if args.engine == "pairs":
+        h.set_engine(nat.ENGINE_PAIRS, 0, 0)
+    else:
+        h.set_engine(nat.ENGINE_STAGED, args.tile_bits, 0)
     h.set_circuit(circuit)
     info = h.plan_info()
     stream = torch.cuda.current_stream(device)
@@ -261,7 +266,8 @@ def run_ours(args):
                 traffic = float(ln.split("=")[1])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "kernel": "k_staged<double,12> (one read+write of the 16 GiB state per launch)",
+                "kernel": ("k_pairs (FP64 mma.sync two-qubit blocks)" if args.engine == "pairs"
+                           else "k_staged<double,12>") + " (one read+write of the 16 GiB state per launch)",
                 "peak_source": f"{peak_kind} hbm_gbs",
                 "per_launch_bytes": per_launch_bytes, "launches_per_step": passes,
                 "gate_model_gbs": info.model_bytes / (ms_per_step / 1e3) / 1e9}
@@ -290,7 +296,7 @@ def run_ours(args):
         "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n_qubits": nq, "depth": DEPTH, "gates": n_gates,
-                   "seed": SEED, "engine": "staged", "tile_bits": int(info.tile_bits),
+                   "seed": SEED, "engine": args.engine, "tile_bits": int(info.tile_bits),
                    "passes": passes, "parallelism": f"replicas x{world}",
                    "l2": "16 GiB state > 126 MB L2: every step streams from HBM, no flush"},
         "roofline": roofline,

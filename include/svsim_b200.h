@@ -46,7 +46,9 @@ typedef enum svb_engine {
     SVB_ENGINE_AUTO = 0,      /* staged for n >= 10, per-gate below */
     SVB_ENGINE_PER_GATE = 1,  /* one HBM sweep per elementary gate, as the reference */
     SVB_ENGINE_STAGED = 2,    /* many gates per HBM sweep through a shared-memory tile */
-    SVB_ENGINE_FUSED = 3      /* gates fused into dense k-qubit blocks (FP32 only) */
+    SVB_ENGINE_FUSED = 3,     /* gates fused into dense k-qubit blocks (FP32 only) */
+    SVB_ENGINE_PAIRS = 4      /* FP64 two-qubit blocks on the FP64 tensor cores (FP64, n >= 12,
+                                 no SRN) */
 } svb_engine;
 
 /* One gate: the fields of the reference's class Gate (svsim_nvgpu_sin.cuh:99-188)

@@ -71,6 +71,12 @@ void free_plan(Sim* s)
     cudaFree(s->dfused.err);
     cudaFree(s->dfused.norm_partial);
     s->dfused = DevFusedBuffers{};
+    cudaFree(s->dpairs.passes);
+    cudaFree(s->dpairs.ops);
+    cudaFree(s->dpairs.layouts);
+    cudaFree(s->dpairs.gates);
+    s->dpairs = DevPairBuffers{};
+    s->pairs = PairPlan{};
     s->fused = FusedPlan{};
     s->eops.clear();
     s->gates.clear();
@@ -151,6 +157,13 @@ svb_status launch_all(Sim* s, cudaStream_t st)
         if (!F.passes.empty()) {
             cudaError_t e = launch_fused_renorm(s->state, n, s->dfused, st);
             if (e != cudaSuccess) return cuda_fail(e, "fused renormalisation");
+        }
+        return SVB_OK;
+    }
+    if (s->engine == SVB_ENGINE_PAIRS) {
+        for (size_t p = 0; p < s->pairs.passes.size(); p++) {
+            cudaError_t e = launch_pair_pass(s->state, n, (int)p, s->dpairs, st);
+            if (e != cudaSuccess) return cuda_fail(e, "pair pass launch");
         }
         return SVB_OK;
     }
@@ -295,10 +308,12 @@ svb_status svb_reset_state(svb_sim* s)
 svb_status svb_set_engine(svb_sim* s, int engine, int tile_bits, int fusion_width)
 {
     if (!s) return invalid("svb_set_engine: NULL handle");
-    if (engine < SVB_ENGINE_AUTO || engine > SVB_ENGINE_FUSED)
+    if (engine < SVB_ENGINE_AUTO || engine > SVB_ENGINE_PAIRS)
         return invalid("svb_set_engine: unknown engine");
     if (engine == SVB_ENGINE_FUSED && s->precision != SVB_FP32)
         return invalid("svb_set_engine: the fused engine runs FP32 states");
+    if (engine == SVB_ENGINE_PAIRS && s->precision != SVB_FP64)
+        return invalid("svb_set_engine: the pair engine runs FP64 states");
     if (tile_bits != 0 && !staged_supported(s->precision, tile_bits))
         return invalid("svb_set_engine: tile_bits must be 10..12 (FP64) or 11..13 (FP32)");
     if (fusion_width != 0 && (fusion_width < FT_MIN_K || fusion_width > FT_MAX_K))
@@ -356,6 +371,16 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
             return SVB_ERR_UNSUPPORTED;
         }
     }
+    if (engine == SVB_ENGINE_PAIRS) {
+        if (s->precision != SVB_FP64 || n < PR_TILE_BITS) {
+            set_error("svb_set_circuit: the pair engine needs an FP64 state of >= 12 qubits");
+            return SVB_ERR_UNSUPPORTED;
+        }
+        if (!fusable(s->eops)) {
+            set_error("svb_set_circuit: SRN is not complex-linear and has no matrix for the pair engine");
+            return SVB_ERR_UNSUPPORTED;
+        }
+    }
     if (engine == SVB_ENGINE_STAGED && !(staged_supported(s->precision, M) && n >= M)) {
         set_error("svb_set_circuit: the staged engine needs n_qubits >= tile bits (10 FP64, 11 FP32)");
         return SVB_ERR_UNSUPPORTED;
@@ -397,6 +422,36 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
                              F.gates.size() * sizeof(float);
         // one read + write per pass, then the renormalisation (two reads, one write)
         s->info.moved_bytes = 2.0 * sb * (double)F.passes.size() + (F.passes.empty() ? 0.0 : 3.0 * sb);
+    } else if (engine == SVB_ENGINE_PAIRS) {
+        if (!plan_pairs(s->eops, n, s->pairs)) {
+            set_error("svb_set_circuit: the pair planner rejected the circuit");
+            return SVB_ERR_UNSUPPORTED;
+        }
+        const PairPlan& R = s->pairs;
+        SVB_CUDA(cudaMalloc(&s->dpairs.passes, std::max<size_t>(1, R.passes.size()) * sizeof(PairPass)),
+                 "cudaMalloc(plan)");
+        SVB_CUDA(cudaMalloc(&s->dpairs.ops, std::max<size_t>(1, R.ops.size()) * sizeof(PairOp)), "cudaMalloc(plan)");
+        SVB_CUDA(cudaMalloc(&s->dpairs.layouts, std::max<size_t>(1, R.layouts.size()) * sizeof(DevStage)),
+                 "cudaMalloc(plan)");
+        SVB_CUDA(cudaMalloc(&s->dpairs.gates, std::max<size_t>(2, R.gates.size()) * sizeof(double)),
+                 "cudaMalloc(plan)");
+        if (!R.passes.empty())
+            SVB_CUDA(cudaMemcpy(s->dpairs.passes, R.passes.data(), R.passes.size() * sizeof(PairPass),
+                                cudaMemcpyHostToDevice), "plan upload");
+        if (!R.ops.empty())
+            SVB_CUDA(cudaMemcpy(s->dpairs.ops, R.ops.data(), R.ops.size() * sizeof(PairOp), cudaMemcpyHostToDevice),
+                     "plan upload");
+        if (!R.layouts.empty())
+            SVB_CUDA(cudaMemcpy(s->dpairs.layouts, R.layouts.data(), R.layouts.size() * sizeof(DevStage),
+                                cudaMemcpyHostToDevice), "plan upload");
+        if (!R.gates.empty())
+            SVB_CUDA(cudaMemcpy(s->dpairs.gates, R.gates.data(), R.gates.size() * sizeof(double),
+                                cudaMemcpyHostToDevice), "plan upload");
+        s->info.n_passes = R.passes.size();
+        s->info.tile_bits = PR_TILE_BITS;
+        s->info.plan_bytes = R.passes.size() * sizeof(PairPass) + R.ops.size() * sizeof(PairOp) +
+                             R.layouts.size() * sizeof(DevStage) + R.gates.size() * sizeof(double);
+        s->info.moved_bytes = 2.0 * sb * (double)R.passes.size();
     } else if (engine == SVB_ENGINE_STAGED) {
         const int G = s->precision == SVB_FP64 ? 3 : 4;
         plan_staged(s->eops, n, M, G, s->staged);

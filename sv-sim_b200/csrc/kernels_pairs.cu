@@ -1,0 +1,192 @@
+// Pair engine kernel: FP64 two-qubit blocks on the FP64 tensor cores (mma.sync m8n8k4).
+//
+// One launch per pass (pairs.cpp).  Persistent CTAs of 256 threads each take tiles of
+// 4,096 amplitudes; a thread keeps 16 complex<double> in registers.  In the current
+// layout lane bits 0 and 1 hold the block's two qubits, so the four lanes t with equal
+// t >> 2 hold the four amplitudes a = t & 3 of one "vector", and the 8 lane groups of a
+// warp hold 8 vectors.  For every register slot the block is two MMAs,
+//     D^T = X^T G'^T :  d = mma(re, B0, 0);  d = mma(im, B1, d)
+// (A fragment = the thread's real or imaginary part, k-step 0 / 1; B = the lane's two
+// entries of the real 8x8 form G'), and the 2 accumulator registers a thread gets back are
+// the real and imaginary part of its own output amplitude a' = t & 3.  So the tile never
+// leaves the registers between blocks on the same pair.  A PO_SWAP exchanges a lane bit
+// with a register bit by one warp shuffle per moved word; a PO_RELAYOUT sends the tile
+// through shared memory with the staged engine's XOR swizzle.
+#include "staged_core.cuh"
+
+namespace svb {
+namespace {
+
+constexpr int PR_THREADS = 1 << (PR_TILE_BITS - RB);    // 256
+constexpr int PR_NR = 1 << RB;                          // 16
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b, double c0, double c1)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};"
+                 : "=d"(d0), "=d"(d1)
+                 : "d"(a), "d"(b), "d"(c0), "d"(c1));
+}
+
+// exchange lane bit L with register bit R: the element at (lane bit i, register bit j)
+// becomes the one that was at (lane bit j, register bit i)
+template <int L, int R>
+__device__ __forceinline__ void swap_lr(double2* v)
+{
+    const bool hi = (threadIdx.x >> L) & 1;
+#pragma unroll
+    for (int k = 0; k < PR_NR; k++) {
+        if (k & (1 << R)) continue;
+        const int k1 = k | (1 << R);
+        const double2 send = hi ? v[k] : v[k1];
+        double2 recv;
+        recv.x = __shfl_xor_sync(0xffffffffu, send.x, 1 << L);
+        recv.y = __shfl_xor_sync(0xffffffffu, send.y, 1 << L);
+        if (hi) v[k] = recv;
+        else v[k1] = recv;
+    }
+}
+
+template <int L>
+__device__ __forceinline__ void swap_l(double2* v, int r)
+{
+    switch (r) {
+    case 0: swap_lr<L, 0>(v); break;
+    case 1: swap_lr<L, 1>(v); break;
+    case 2: swap_lr<L, 2>(v); break;
+    default: swap_lr<L, 3>(v); break;
+    }
+}
+
+__device__ __forceinline__ void swap_any(double2* v, int lane, int r)
+{
+    switch (lane) {
+    case 0: swap_l<0>(v, r); break;
+    case 1: swap_l<1>(v, r); break;
+    case 2: swap_l<2>(v, r); break;
+    case 3: swap_l<3>(v, r); break;
+    default: swap_l<4>(v, r); break;
+    }
+}
+
+struct PairGOffs {
+    uint64_t thr;
+    uint64_t reg[RB];
+};
+
+__device__ __forceinline__ void pair_goffs(const DevStage& S, const uint8_t* local_q, int tid, PairGOffs& g)
+{
+    uint64_t t = 0;
+#pragma unroll
+    for (int b = 0; b < PR_TILE_BITS - RB; b++)
+        if ((tid >> b) & 1) t |= 1ull << local_q[S.thr_pos[b]];
+    g.thr = t;
+#pragma unroll
+    for (int i = 0; i < RB; i++) g.reg[i] = 1ull << local_q[S.reg_pos[i]];
+}
+
+__device__ __forceinline__ uint64_t pair_goff(const PairGOffs& g, int k)
+{
+    uint64_t r = g.thr;
+#pragma unroll
+    for (int i = 0; i < RB; i++)
+        if ((k >> i) & 1) r |= g.reg[i];
+    return r;
+}
+
+__device__ __forceinline__ PairOp load_op(const PairOp* p)
+{
+    const uint4 w = __ldg(reinterpret_cast<const uint4*>(p));
+    PairOp o;
+    *reinterpret_cast<uint4*>(&o) = w;
+    return o;
+}
+
+__global__ void __launch_bounds__(PR_THREADS, 2)
+k_pairs(double2* __restrict__ sv, const PairPass* __restrict__ passes, const PairOp* __restrict__ ops,
+        const DevStage* __restrict__ layouts, const double2* __restrict__ gates, int pass_index,
+        uint64_t tiles)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    __shared__ PairPass sP;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(passes + pass_index);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sP);
+        for (int w = tid; w < (int)(sizeof(PairPass) / 4); w += PR_THREADS) dst[w] = src[w];
+        __syncthreads();
+    }
+    const PairPass& P = sP;
+    const int ob = P.op_begin, oe = P.op_end;
+    PairGOffs gin, gout;
+    pair_goffs(layouts[P.load_layout], P.local_q, tid, gin);
+    pair_goffs(layouts[P.store_layout], P.local_q, tid, gout);
+
+    for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        uint64_t base = 0;
+        for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
+        double2 v[PR_NR];
+#pragma unroll
+        for (int k = 0; k < PR_NR; k++) v[k] = sv[base | pair_goff(gin, k)];
+        for (int o = ob; o < oe; o++) {
+            const PairOp op = load_op(ops + o);
+            if (op.kind == PO_BLOCK) {
+                int var = 0;
+                for (int c = 0; c < op.ncond; c++) var |= (int)((base >> op.cond_q[c]) & 1ull) << c;
+                const double2 g = __ldg(gates + (size_t)(op.gate + var) * 32 + lane);
+#pragma unroll
+                for (int k = 0; k < PR_NR; k++) {
+                    double d0, d1;
+                    dmma(d0, d1, v[k].x, g.x, 0.0, 0.0);
+                    dmma(d0, d1, v[k].y, g.y, d0, d1);
+                    v[k].x = d0;
+                    v[k].y = d1;
+                }
+            } else if (op.kind == PO_SWAP) {
+                swap_any(v, op.lane, op.reg);
+            } else {
+                Slots from, to;
+                make_slots<double, PR_TILE_BITS - RB>(layouts[op.src], tid, from);
+                make_slots<double, PR_TILE_BITS - RB>(layouts[op.layout], tid, to);
+#pragma unroll
+                for (int k = 0; k < PR_NR; k++) sm[slot_of(from, k)] = v[k];
+                __syncthreads();
+#pragma unroll
+                for (int k = 0; k < PR_NR; k++) v[k] = sm[slot_of(to, k)];
+                __syncthreads();
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < PR_NR; k++) sv[base | pair_goff(gout, k)] = v[k];
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_pair_pass(void* state, int n, int pass_index, const DevPairBuffers& b, cudaStream_t s)
+{
+    static int max_ctas[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t smem = sizeof(double2) << PR_TILE_BITS;
+    if (dev < 64 && max_ctas[dev] == 0) {
+        cudaError_t e = cudaFuncSetAttribute(k_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs, PR_THREADS, smem);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        max_ctas[dev] = (per_sm > 0 ? per_sm : 1) * sms;
+    }
+    if (n < PR_TILE_BITS) return cudaErrorInvalidValue;
+    const uint64_t tiles = 1ull << (n - PR_TILE_BITS);
+    uint64_t grid = tiles;
+    if (dev < 64 && grid > (uint64_t)max_ctas[dev]) grid = (uint64_t)max_ctas[dev];
+    k_pairs<<<(unsigned)grid, PR_THREADS, smem, s>>>(static_cast<double2*>(state), b.passes, b.ops, b.layouts,
+                                                     reinterpret_cast<const double2*>(b.gates), pass_index, tiles);
+    return cudaGetLastError();
+}
+
+}  // namespace svb

@@ -1,0 +1,549 @@
+// Planner of the pair engine (FP64 two-qubit blocks on the FP64 tensor cores).
+//
+// Passes are cut exactly as for the staged engine (select_passes).  Inside a pass the
+// elementary ops, in program order, are folded into two-qubit blocks:
+//   * a one-qubit op (dense or diagonal) on a local qubit p is multiplied into pend[p],
+//     a pending 2x2 matrix, and applied with the next block that touches p;
+//   * a CX on two local qubits (c, t) closes pend[c] and pend[t] into one block,
+//     CX . (pend[c] (x) pend[t]);
+//   * a CX whose control is not local is an X on t for the tiles where that qubit is 1:
+//     pend[t] gets a variant per value of the control (a condition qubit);
+//   * a diagonal op on a non-local qubit is a phase for the tiles where that qubit is 1
+//     (or 0, for the general diagonal): it is folded into a block as a scalar variant.
+// Blocks on other qubits commute with a pending one-qubit matrix, so deferring it keeps
+// the circuit's meaning; blocks that share a qubit keep their program order, and blocks on
+// disjoint pairs are taken in the order that needs the fewest moves.  At the end of the pass
+// the remaining pending matrices are closed in pairs.  A block carries at most
+// PR_MAX_COND condition qubits (4 variants); merges that would exceed it close the
+// pending matrix first.
+//
+// Each block needs its two qubits on lane bits 0 and 1.  The layout planner follows the
+// blocks: a qubit held in a register bit is swapped onto the lane with one warp shuffle
+// exchange (PO_SWAP), a qubit on another lane goes through a register (two exchanges), and
+// a qubit on a warp bit needs a shared-memory redistribution (PO_RELAYOUT) whose new
+// layout keeps the soonest-needed qubits on lanes and registers.  A pass is loaded and
+// stored with its 5 lowest local positions on the lanes (coalesced 128-byte runs).
+//
+// The device form of a block variant is its real 8x8 matrix G'[r][kk] with rows
+// r = 2a' + re/im of the output amplitude and columns kk = a (real part) or 4 + a
+// (imaginary part) of the input amplitude, stored as 32 lanes x (G'[t>>2][t&3],
+// G'[t>>2][4 + (t&3)]): the B fragments of the two k-steps of the MMA D^T = X^T G'^T.
+#include <algorithm>
+#include <array>
+#include <complex>
+#include <cstring>
+
+#include "gate_math.cuh"
+
+namespace svb {
+namespace {
+
+using cplx = std::complex<double>;
+using M2 = std::array<cplx, 4>;     // row-major 2x2
+using M4 = std::array<cplx, 16>;    // row-major 4x4, index a = bit0 + 2 bit1
+
+constexpr int NSLOT = PR_TILE_BITS;  // 0..4 lanes, 5..8 registers, 9..11 warps
+constexpr int SLOT_REG = PR_LANE_BITS;
+constexpr int SLOT_WARP = PR_LANE_BITS + RB;
+
+M2 ident2() { return M2{cplx(1), cplx(0), cplx(0), cplx(1)}; }
+M4 ident4()
+{
+    M4 m{};
+    for (int i = 0; i < 4; i++) m[i * 5] = 1;
+    return m;
+}
+M2 mul2(const M2& a, const M2& b)
+{
+    M2 r{};
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) r[i * 2 + j] = a[i * 2] * b[j] + a[i * 2 + 1] * b[2 + j];
+    return r;
+}
+M4 mul4(const M4& a, const M4& b)
+{
+    M4 r{};
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            cplx s = 0;
+            for (int k = 0; k < 4; k++) s += a[i * 4 + k] * b[k * 4 + j];
+            r[i * 4 + j] = s;
+        }
+    return r;
+}
+// P0 on bit 0, P1 on bit 1
+M4 kron(const M2& p0, const M2& p1)
+{
+    M4 r{};
+    for (int ap = 0; ap < 4; ap++)
+        for (int a = 0; a < 4; a++)
+            r[ap * 4 + a] = p0[(ap & 1) * 2 + (a & 1)] * p1[(ap >> 1) * 2 + (a >> 1)];
+    return r;
+}
+// the same operator with the roles of bit 0 and bit 1 exchanged
+M4 swap_bits(const M4& m)
+{
+    auto s = [](int a) { return ((a & 1) << 1) | (a >> 1); };
+    M4 r{};
+    for (int ap = 0; ap < 4; ap++)
+        for (int a = 0; a < 4; a++) r[s(ap) * 4 + s(a)] = m[ap * 4 + a];
+    return r;
+}
+
+// 2x2 matrix of an elementary op, read off the kernels' own expressions on the basis
+M2 matrix_of(const EOp& e)
+{
+    const Coef<double> c = load_coef<double>(e.m);
+    M2 u{};
+    for (int col = 0; col < 2; col++) {
+        double2 a0 = make_double2(col == 0 ? 1.0 : 0.0, 0.0), a1 = make_double2(col == 1 ? 1.0 : 0.0, 0.0);
+        if (form_is_diag(e.form)) {
+            diag_one<double>(e.form, c, a1);
+            if (e.form == F_DIAG) diag_zero<double>(e.form, c, a0);
+        } else {
+            dense_pair<double>(e.form, c, a0, a1);
+        }
+        u[col] = cplx(a0.x, a0.y);
+        u[2 + col] = cplx(a1.x, a1.y);
+    }
+    return u;
+}
+
+// condition qubits -> variants (variant index bit i = value of cond[i] in the tile)
+std::vector<int> cond_union(const std::vector<int>& a, const std::vector<int>& b)
+{
+    std::vector<int> u = a;
+    for (int q : b)
+        if (std::find(u.begin(), u.end(), q) == u.end()) u.push_back(q);
+    return u;
+}
+int sub_index(const std::vector<int>& uni, int u, const std::vector<int>& sub)
+{
+    int r = 0;
+    for (size_t i = 0; i < sub.size(); i++) {
+        const int j = (int)(std::find(uni.begin(), uni.end(), sub[i]) - uni.begin());
+        r |= ((u >> j) & 1) << i;
+    }
+    return r;
+}
+
+struct Pend {                       // conditional 2x2 on one local position
+    bool active = false;
+    std::vector<int> cond;
+    std::vector<M2> v{ident2()};
+};
+struct Scalar {                     // conditional phase of the whole tile
+    bool active = false;
+    std::vector<int> cond;
+    std::vector<cplx> v{cplx(1)};
+};
+struct Block {
+    int x, y;                        // local positions: bit 0 = x, bit 1 = y
+    std::vector<int> cond;
+    std::vector<M4> v;
+};
+
+// pend = u(cond) . pend
+void pend_apply(Pend& p, const std::vector<int>& ucond, const std::vector<M2>& uv)
+{
+    const std::vector<int> uni = cond_union(p.cond, ucond);
+    std::vector<M2> nv((size_t)1 << uni.size());
+    for (size_t u = 0; u < nv.size(); u++)
+        nv[u] = mul2(uv[sub_index(uni, (int)u, ucond)], p.v[sub_index(uni, (int)u, p.cond)]);
+    p.cond = uni;
+    p.v = nv;
+    p.active = true;
+}
+
+struct PassPairs {
+    std::vector<Block> blocks;
+    Pend pend[NSLOT];
+    Scalar ph;
+
+    // block = after . (pend[x] (x) pend[y]), plus the pending tile phase when it fits
+    void close(int x, int y, const M4* after)
+    {
+        Block b;
+        b.x = x;
+        b.y = y;
+        b.cond = cond_union(pend[x].cond, pend[y].cond);
+        const bool with_ph = ph.active && cond_union(b.cond, ph.cond).size() <= (size_t)PR_MAX_COND;
+        if (with_ph) b.cond = cond_union(b.cond, ph.cond);
+        b.v.resize((size_t)1 << b.cond.size());
+        for (size_t u = 0; u < b.v.size(); u++) {
+            M4 m = kron(pend[x].v[sub_index(b.cond, (int)u, pend[x].cond)],
+                        pend[y].v[sub_index(b.cond, (int)u, pend[y].cond)]);
+            if (after) m = mul4(*after, m);
+            if (with_ph) {
+                const cplx s = ph.v[sub_index(b.cond, (int)u, ph.cond)];
+                for (auto& z : m) z *= s;
+            }
+            b.v[u] = m;
+        }
+        if (with_ph) ph = Scalar{};
+        pend[x] = Pend{};
+        pend[y] = Pend{};
+        blocks.push_back(b);
+    }
+    int partner_of(int p) const { return p == 0 ? 1 : 0; }
+    // closes pend[p] alone (with an idle partner)
+    void flush(int p)
+    {
+        int q = partner_of(p);
+        for (int k = 0; k < NSLOT; k++)
+            if (k != p && !pend[k].active) { q = k; break; }
+        if (pend[q].active && cond_union(pend[p].cond, pend[q].cond).size() > (size_t)PR_MAX_COND) {
+            Pend keep = pend[q];
+            pend[q] = Pend{};
+            close(p, q, nullptr);
+            pend[q] = keep;
+        } else {
+            close(p, q, nullptr);
+        }
+    }
+    void add_1q(int p, const std::vector<int>& ucond, const std::vector<M2>& uv)
+    {
+        if (cond_union(pend[p].cond, ucond).size() > (size_t)PR_MAX_COND) flush(p);
+        pend_apply(pend[p], ucond, uv);
+    }
+    void add_phase(int q, const cplx& f0, const cplx& f1)
+    {
+        if (ph.active && cond_union(ph.cond, {q}).size() > (size_t)PR_MAX_COND) {
+            // close the tile phase on its own before it outgrows a block
+            Pend a = pend[0], b = pend[1];
+            pend[0] = Pend{};
+            pend[1] = Pend{};
+            close(0, 1, nullptr);
+            pend[0] = a;
+            pend[1] = b;
+        }
+        const std::vector<int> uni = cond_union(ph.cond, {q});
+        std::vector<cplx> nv((size_t)1 << uni.size());
+        for (size_t u = 0; u < nv.size(); u++) {
+            const int bitq = sub_index(uni, (int)u, {q});
+            nv[u] = ph.v[sub_index(uni, (int)u, ph.cond)] * (bitq ? f1 : f0);
+        }
+        ph.cond = uni;
+        ph.v = nv;
+        ph.active = true;
+    }
+    void add_cx(int c, int t)
+    {
+        if (cond_union(pend[c].cond, pend[t].cond).size() > (size_t)PR_MAX_COND) flush(c);
+        M4 cx{};
+        for (int a = 0; a < 4; a++) {
+            const int ap = (a & 1) ? (a ^ 2) : a;     // bit 0 = control, bit 1 = target
+            cx[ap * 4 + a] = 1;
+        }
+        close(c, t, &cx);
+    }
+    void finish()
+    {
+        std::vector<int> open;
+        for (int p = 0; p < NSLOT; p++)
+            if (pend[p].active) open.push_back(p);
+        size_t i = 0;
+        while (i + 1 < open.size()) {
+            const int a = open[i], b = open[i + 1];
+            if (cond_union(pend[a].cond, pend[b].cond).size() <= (size_t)PR_MAX_COND) {
+                close(a, b, nullptr);
+                i += 2;
+            } else {
+                flush(a);
+                i += 1;
+            }
+        }
+        if (i < open.size()) flush(open[i]);
+        if (ph.active) flush(0);       // pend[0] is idle here: a block with only the phase
+    }
+};
+
+struct LayoutPlanner {
+    PairPlan& plan;
+    int slot_pos[NSLOT];
+    int where[NSLOT];
+    bool dry = false;                // only follow the layout (for trying block orders)
+
+    DevStage stage() const
+    {
+        DevStage st;
+        std::memset(&st, 0, sizeof(st));
+        for (int i = 0; i < RB; i++) st.reg_pos[i] = (uint8_t)slot_pos[SLOT_REG + i];
+        for (int b = 0; b < PR_LANE_BITS; b++) st.thr_pos[b] = (uint8_t)slot_pos[b];
+        for (int w = 0; w < NSLOT - SLOT_WARP; w++) st.thr_pos[PR_LANE_BITS + w] = (uint8_t)slot_pos[SLOT_WARP + w];
+        return st;
+    }
+    int push_layout()
+    {
+        plan.layouts.push_back(stage());
+        return (int)plan.layouts.size() - 1;
+    }
+    void set(const int* sp)
+    {
+        for (int s = 0; s < NSLOT; s++) {
+            slot_pos[s] = sp[s];
+            where[sp[s]] = s;
+        }
+    }
+    void swap_lr(int lane, int reg)
+    {
+        if (!dry) {
+            PairOp op;
+            std::memset(&op, 0, sizeof(op));
+            op.kind = PO_SWAP;
+            op.lane = (uint8_t)lane;
+            op.reg = (uint8_t)reg;
+            plan.ops.push_back(op);
+            plan.n_swaps++;
+        }
+        const int a = slot_pos[lane], b = slot_pos[SLOT_REG + reg];
+        slot_pos[lane] = b;
+        slot_pos[SLOT_REG + reg] = a;
+        where[b] = lane;
+        where[a] = SLOT_REG + reg;
+    }
+    void relayout(const int* sp)
+    {
+        if (dry) {
+            set(sp);
+            return;
+        }
+        PairOp op;
+        std::memset(&op, 0, sizeof(op));
+        op.kind = PO_RELAYOUT;
+        op.src = (uint16_t)push_layout();
+        set(sp);
+        op.layout = (uint16_t)push_layout();
+        plan.ops.push_back(op);
+        plan.n_relayouts++;
+    }
+    // the register whose qubit is needed last
+    int spare_reg(const std::vector<int>& next_use) const
+    {
+        int best = 0;
+        for (int r = 1; r < RB; r++)
+            if (next_use[slot_pos[SLOT_REG + r]] > next_use[slot_pos[SLOT_REG + best]]) best = r;
+        return best;
+    }
+    void move_to_lane(int pos, int lane, const std::vector<int>& next_use)
+    {
+        const int s = where[pos];
+        if (s == lane) return;
+        if (s >= SLOT_REG && s < SLOT_WARP) {
+            swap_lr(lane, s - SLOT_REG);
+            return;
+        }
+        const int r = spare_reg(next_use);      // another lane: through a register
+        swap_lr(s, r);
+        swap_lr(lane, r);
+    }
+    // a layout with x, y on lanes 0, 1 and the other positions by next use
+    void relayout_for(int x, int y, const std::vector<int>& next_use)
+    {
+        std::vector<int> rest;
+        for (int p = 0; p < NSLOT; p++)
+            if (p != x && p != y) rest.push_back(p);
+        std::stable_sort(rest.begin(), rest.end(), [&](int a, int b) { return next_use[a] < next_use[b]; });
+        int sp[NSLOT];
+        sp[0] = x;
+        sp[1] = y;
+        // lane 2: a position whose residue mod 3 differs from x's and y's, so the three
+        // lowest lane bits hit distinct swizzle groups (conflict-free shared-memory
+        // phases); taken from the latest-needed end, the rest by next use
+        int l2 = -1;
+        for (int i = (int)rest.size() - 1; i >= 0 && l2 < 0; i--)
+            if (rest[i] % 3 != x % 3 && rest[i] % 3 != y % 3) l2 = i;
+        if (l2 < 0) l2 = (int)rest.size() - 1;
+        sp[2] = rest[l2];
+        rest.erase(rest.begin() + l2);
+        // soonest-needed in registers (one exchange away), then lanes 3..4, warps last
+        int k = 0;
+        for (int r = 0; r < RB; r++) sp[SLOT_REG + r] = rest[k++];
+        for (int l = 3; l < PR_LANE_BITS; l++) sp[l] = rest[k++];
+        for (int w = SLOT_WARP; w < NSLOT; w++) sp[w] = rest[k++];
+        relayout(sp);
+    }
+    // exchanges needed to bring `pos` onto a target lane (a warp bit: a relayout)
+    int cost_of(int pos) const
+    {
+        const int s = where[pos];
+        if (s <= 1) return 0;
+        if (s >= SLOT_REG && s < SLOT_WARP) return 1;
+        if (s < SLOT_REG) return 2;
+        return 8;
+    }
+    int pair_cost(int x, int y) const
+    {
+        const int sx = where[x], sy = where[y];
+        if ((sx == 0 && sy == 1) || (sx == 1 && sy == 0)) return 0;
+        return cost_of(x) + cost_of(y);
+    }
+    void ensure(int x, int y, const std::vector<int>& next_use)
+    {
+        const int sx = where[x], sy = where[y];
+        if ((sx == 0 && sy == 1) || (sx == 1 && sy == 0)) return;
+        if (sx >= SLOT_WARP || sy >= SLOT_WARP) {
+            relayout_for(x, y, next_use);
+            return;
+        }
+        if (sy == 0 || sx == 1) std::swap(x, y);
+        move_to_lane(x, 0, next_use);
+        move_to_lane(y, 1, next_use);
+    }
+};
+
+void write_block(PairPlan& plan, const Block& b, bool transposed)
+{
+    for (const M4& m0 : b.v) {
+        const M4 m = transposed ? swap_bits(m0) : m0;
+        double g[8][8];
+        for (int ap = 0; ap < 4; ap++)
+            for (int a = 0; a < 4; a++) {
+                const cplx z = m[ap * 4 + a];
+                g[2 * ap][a] = z.real();
+                g[2 * ap + 1][a] = z.imag();
+                g[2 * ap][4 + a] = -z.imag();
+                g[2 * ap + 1][4 + a] = z.real();
+            }
+        for (int t = 0; t < 32; t++) {
+            plan.gates.push_back(g[t >> 2][t & 3]);
+            plan.gates.push_back(g[t >> 2][4 + (t & 3)]);
+        }
+    }
+}
+
+}  // namespace
+
+bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan)
+{
+    plan = PairPlan{};
+    if (n < PR_TILE_BITS) return false;
+    for (const EOp& e : ops)
+        if (e.form == F_SRN) return false;      // only real-linear: not a matrix
+    select_passes(ops, n, PR_TILE_BITS, 3, [&](uint64_t L, const std::vector<int>& taken) {
+        PairPass P;
+        std::memset(&P, 0, sizeof(P));
+        int pos_of[64];
+        for (int q = 0; q < 64; q++) pos_of[q] = -1;
+        int nl = 0, nn = 0;
+        for (int q = 0; q < n; q++) {
+            if ((L >> q) & 1) { pos_of[q] = nl; P.local_q[nl++] = (uint8_t)q; }
+            else P.nonlocal_q[nn++] = (uint8_t)q;
+        }
+        P.n_nonlocal = nn;
+        // 1. blocks
+        PassPairs pp;
+        for (int i : taken) {
+            const EOp& e = ops[i];
+            if (e.form == F_CX) {
+                const int t = pos_of[e.q], c = pos_of[e.c];
+                if (c >= 0) {
+                    pp.add_cx(c, t);
+                } else {
+                    const M2 x{cplx(0), cplx(1), cplx(1), cplx(0)};
+                    pp.add_1q(t, {(int)e.c}, {ident2(), x});
+                }
+            } else if (pos_of[e.q] >= 0) {
+                pp.add_1q(pos_of[e.q], {}, {matrix_of(e)});
+            } else {
+                const M2 d = matrix_of(e);             // diagonal op on a tile qubit
+                pp.add_phase((int)e.q, d[0], d[3]);
+            }
+        }
+        pp.finish();
+        // 2. layouts: next use of every position after each block
+        const size_t nb = pp.blocks.size();
+        const int INF = 1 << 30;
+        std::vector<std::vector<int>> next(nb + 1, std::vector<int>(NSLOT, INF));
+        for (size_t i = nb; i-- > 0;) {
+            next[i] = next[i + 1];
+            next[i][pp.blocks[i].x] = (int)i;
+            next[i][pp.blocks[i].y] = (int)i;
+        }
+        LayoutPlanner lp{plan, {}, {}};
+        int sp[NSLOT];
+        for (int l = 0; l < PR_LANE_BITS; l++) sp[l] = l;     // the 5 lowest positions on lanes
+        std::vector<int> rest;
+        for (int p = PR_LANE_BITS; p < NSLOT; p++) rest.push_back(p);
+        std::stable_sort(rest.begin(), rest.end(), [&](int a, int b) { return next[0][a] < next[0][b]; });
+        for (int k = 0; k < (int)rest.size(); k++) sp[SLOT_REG + k] = rest[k];
+        lp.set(sp);
+        P.load_layout = lp.push_layout();
+        P.op_begin = (int32_t)plan.ops.size();
+        // blocks on disjoint pairs commute: take them in an order that needs few moves.
+        // Block j may go once every earlier block sharing a qubit with it has gone.
+        std::vector<int> order;
+        {
+            std::vector<char> done(nb, 0);
+            LayoutPlanner probe = lp;
+            probe.dry = true;
+            size_t first = 0;
+            for (size_t step = 0; step < nb; step++) {
+                while (first < nb && done[first]) first++;
+                int best = -1, best_cost = 1 << 30;
+                uint32_t busy = 0;            // qubits of skipped blocks (to keep order)
+                for (size_t j = first; j < nb && j < first + 48; j++) {
+                    if (done[j]) continue;
+                    const uint32_t m = (1u << pp.blocks[j].x) | (1u << pp.blocks[j].y);
+                    if (m & busy) { busy |= m; continue; }
+                    const int c = probe.pair_cost(pp.blocks[j].x, pp.blocks[j].y);
+                    if (c < best_cost) { best_cost = c; best = (int)j; }
+                    busy |= m;
+                    if (c == 0) break;
+                }
+                done[best] = 1;
+                order.push_back(best);
+                // advance the probe layout as the real planner will (next use in
+                // program order is a close stand-in for the final order's)
+                probe.ensure(pp.blocks[best].x, pp.blocks[best].y, next[best]);
+            }
+        }
+        // next use in the chosen order
+        std::vector<std::vector<int>> nxt(nb + 1, std::vector<int>(NSLOT, INF));
+        for (size_t i = nb; i-- > 0;) {
+            nxt[i] = nxt[i + 1];
+            nxt[i][pp.blocks[order[i]].x] = (int)i;
+            nxt[i][pp.blocks[order[i]].y] = (int)i;
+        }
+        for (size_t oi = 0; oi < nb; oi++) {
+            const Block& b = pp.blocks[order[oi]];
+            lp.ensure(b.x, b.y, nxt[oi]);
+            PairOp op;
+            std::memset(&op, 0, sizeof(op));
+            op.kind = PO_BLOCK;
+            op.ncond = (uint8_t)b.cond.size();
+            for (size_t c = 0; c < b.cond.size(); c++) op.cond_q[c] = (uint8_t)b.cond[c];
+            op.gate = (uint32_t)(plan.gates.size() / 64);
+            write_block(plan, b, lp.slot_pos[0] != b.x);
+            plan.ops.push_back(op);
+            plan.n_blocks++;
+        }
+        // 3. back to a storable layout: the 5 lowest positions on the lanes
+        bool warp_low = false;
+        for (int p = 0; p < PR_LANE_BITS; p++)
+            if (lp.where[p] >= SLOT_WARP) warp_low = true;
+        if (warp_low) {
+            int canon[NSLOT];
+            std::memcpy(canon, sp, sizeof(canon));
+            lp.relayout(canon);
+        } else {
+            for (int l = 0; l < PR_LANE_BITS; l++) {
+                if (lp.slot_pos[l] < PR_LANE_BITS) continue;
+                for (int p = 0; p < PR_LANE_BITS; p++) {
+                    const int s = lp.where[p];
+                    if (s >= SLOT_REG && s < SLOT_WARP) {
+                        lp.swap_lr(l, s - SLOT_REG);
+                        break;
+                    }
+                }
+            }
+        }
+        P.store_layout = lp.push_layout();
+        P.op_end = (int32_t)plan.ops.size();
+        plan.passes.push_back(P);
+        return std::vector<int>{};
+    });
+    return true;
+}
+
+}  // namespace svb

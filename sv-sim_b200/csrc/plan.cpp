@@ -20,6 +20,7 @@
 // holds in registers; between stages the tile is re-distributed through shared memory.
 #include <algorithm>
 #include <cstring>
+#include <functional>
 
 #include "svb_internal.h"
 
@@ -206,20 +207,14 @@ struct PassBuilder {
 
 }  // namespace
 
-void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& plan)
+void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
+                   const std::function<std::vector<int>(uint64_t, const std::vector<int>&)>& build)
 {
-    plan.passes.clear();
-    plan.stages.clear();
-    plan.ops.clear();
-    plan.M = M;
-    plan.G = G;
     const size_t N = ops.size();
     const uint64_t all = (n >= 64) ? ~0ull : (bit(n) - 1);
     std::vector<OpInfo> inf(N);
     for (size_t i = 0; i < N; i++) inf[i] = info_of(ops[i], all);
     const uint64_t low = bit(G) - 1;
-
-    PassBuilder pb{ops, inf, n, M, G, M - RB, plan};
     std::vector<char> done(N, 0);
     std::vector<int> taken;
     size_t first = 0;
@@ -255,8 +250,23 @@ void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& p
         }
         for (int q = 0; nL < M && q < n; q++)
             if (!((L >> q) & 1)) { L |= bit(q); nL++; }
-        for (int i : pb.build(L, taken)) done[i] = 0;
+        for (int i : build(L, taken)) done[i] = 0;
     }
+}
+
+void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& plan)
+{
+    plan.passes.clear();
+    plan.stages.clear();
+    plan.ops.clear();
+    plan.M = M;
+    plan.G = G;
+    const size_t N = ops.size();
+    const uint64_t all = (n >= 64) ? ~0ull : (bit(n) - 1);
+    std::vector<OpInfo> inf(N);
+    for (size_t i = 0; i < N; i++) inf[i] = info_of(ops[i], all);
+    PassBuilder pb{ops, inf, n, M, G, M - RB, plan};
+    select_passes(ops, n, M, G, [&](uint64_t L, const std::vector<int>& taken) { return pb.build(L, taken); });
 }
 
 }  // namespace svb

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstddef>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -119,6 +120,69 @@ struct StagedPlan {
 
 // Builds the staged plan for `ops` on n qubits with tile bits M and low-group G.
 void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& plan);
+
+// ---- pair engine (FP64 two-qubit blocks on the FP64 tensor cores) ----------------
+//
+// A pass holds PR_TILE_BITS = 12 local qubits.  Each of the 256 threads keeps 16
+// amplitudes; the 12 local positions sit on 5 lane bits, 4 register bits and 3 warp
+// bits, described by a DevStage (thr_pos[0..4] = lane bits, thr_pos[5..7] = warp bits,
+// reg_pos = register bits).  A block is a 4x4 complex matrix on the two qubits held by
+// lane bits 0 and 1 (amplitude index a = lane bits 0 + 2 lane bit 1), applied with
+// mma.sync m8n8k4 f64 to every register slot.  Between blocks, lane and register bits
+// are exchanged with warp shuffles, or the tile is redistributed through shared memory.
+constexpr int PR_TILE_BITS = 12;
+constexpr int PR_LANE_BITS = 5;
+constexpr int PR_MAX_COND = 2;          // tile-selected variants: at most 2 non-local qubits
+enum PairOpKind : uint8_t { PO_SWAP = 0, PO_RELAYOUT = 1, PO_BLOCK = 2 };
+
+struct PairOp {                          // 16 bytes
+    uint8_t kind;
+    uint8_t lane;                        // PO_SWAP: lane bit
+    uint8_t reg;                         // PO_SWAP: register bit
+    uint8_t ncond;                       // PO_BLOCK: number of condition qubits
+    uint8_t cond_q[PR_MAX_COND];         // PO_BLOCK: global qubits selecting the variant
+    uint16_t layout;                     // PO_RELAYOUT: target layout
+    uint32_t gate;                       // PO_BLOCK: first variant (units of 32 double2)
+    uint16_t src;                        // PO_RELAYOUT: current layout
+    uint16_t pad;
+};
+
+static_assert(sizeof(PairOp) == 16, "PairOp layout");
+
+struct PairPass {
+    uint8_t local_q[PR_TILE_BITS];
+    uint8_t nonlocal_q[64 - PR_TILE_BITS];
+    int32_t n_nonlocal;
+    int32_t op_begin, op_end;
+    int32_t load_layout, store_layout;
+    int32_t pad;
+};
+
+struct PairPlan {
+    std::vector<PairPass> passes;
+    std::vector<PairOp> ops;
+    std::vector<DevStage> layouts;
+    std::vector<double> gates;           // per variant: 32 lanes x (B0, B1)
+    size_t n_blocks = 0, n_swaps = 0, n_relayouts = 0;
+};
+
+// Builds the pair plan; false if an op cannot be written as a matrix (SRN).
+bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan);
+
+struct DevPairBuffers {
+    PairPass* passes = nullptr;
+    PairOp* ops = nullptr;
+    DevStage* layouts = nullptr;
+    double* gates = nullptr;
+};
+cudaError_t launch_pair_pass(void* state, int n, int pass_index, const DevPairBuffers& b, cudaStream_t s);
+
+// The pass cut shared by the staged and pair planners: ops in program order are taken
+// into a pass of M local qubits (always including the G lowest) while their dense or CX
+// target can be made local and they touch no qubit of an op skipped earlier.  `build`
+// receives each pass's local-qubit mask and ops and returns the ops it could not place.
+void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
+                   const std::function<std::vector<int>(uint64_t, const std::vector<int>&)>& build);
 
 // ---------------------------------------------------------------------------------
 // Fused tensor-core engine (FP32 states): passes of up to FT_MAX_BLOCKS fused k-qubit
@@ -257,6 +321,8 @@ struct Sim {
     DevPlanBuffers dplan;
     FusedPlan fused;
     DevFusedBuffers dfused;
+    PairPlan pairs;
+    DevPairBuffers dpairs;
     bool have_circuit = false;
     cudaGraphExec_t graph = nullptr;
     cudaStream_t capture_stream = nullptr;

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libs
 
 SVB_OK, SVB_ERR_INVALID, SVB_ERR_CUDA, SVB_ERR_OOM, SVB_ERR_UNSUPPORTED, SVB_ERR_STATE = range(6)
 SVB_FP64, SVB_FP32 = 0, 1
-ENGINE_AUTO, ENGINE_PER_GATE, ENGINE_STAGED, ENGINE_FUSED = 0, 1, 2, 3
+ENGINE_AUTO, ENGINE_PER_GATE, ENGINE_STAGED, ENGINE_FUSED, ENGINE_PAIRS = 0, 1, 2, 3, 4
 
 
 class SvbError(RuntimeError):

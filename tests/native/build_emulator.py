@@ -14,7 +14,7 @@ OUT = os.path.join(HERE, "_build", "libstaged_emu.so")
 
 def build() -> str:
     srcs = [os.path.join(HERE, "staged_emulator.cu"), os.path.join(CSRC, "plan.cpp"),
-            os.path.join(CSRC, "lower.cpp"), os.path.join(CSRC, "fuse.cpp")]
+            os.path.join(CSRC, "lower.cpp"), os.path.join(CSRC, "fuse.cpp"), os.path.join(CSRC, "pairs.cpp")]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     if os.path.exists(OUT) and os.path.getmtime(OUT) >= max(os.path.getmtime(d) for d in deps):
         return OUT

@@ -256,3 +256,159 @@ extern "C" int emu_fused_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
     }
     return 0;
 }
+
+// ---- pair engine ---------------------------------------------------------------------
+// Executes a pair plan (pairs.cpp) thread by thread with the kernel's data movement:
+// PO_SWAP as the warp-shuffle exchange, PO_RELAYOUT through the swizzled shared tile
+// (every slot written once), PO_BLOCK as the mma.sync m8n8k4 fragment rules (thread t
+// holds A[t>>2][t&3] and B[t&3][t>>2], receives D[t>>2][2(t&3)], D[t>>2][2(t&3)+1]).
+extern "C" int emu_pairs_run(uint32_t n, const svb_gate* gates, size_t n_gates, double* re, double* im,
+                             uint64_t* stats)
+{
+    std::vector<EOp> eops;
+    for (size_t i = 0; i < n_gates; i++)
+        if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
+    PairPlan plan;
+    if (!plan_pairs(eops, (int)n, plan)) return -6;
+    constexpr int NT = 256, NR = 16, TB = 8;
+    std::vector<double2> sv(1ull << n);
+    for (auto& a : sv) a = make_double2(0, 0);
+    sv[0] = make_double2(1, 0);
+    std::vector<double2> regs((size_t)NT * NR), sm(4096);
+    std::vector<int> written(4096);
+    const uint64_t tiles = 1ull << (n - PR_TILE_BITS);
+    for (const PairPass& P : plan.passes) {
+        auto goff = [&](const DevStage& S, int t, int k) {
+            uint64_t g = 0;
+            for (int b = 0; b < TB; b++)
+                if ((t >> b) & 1) g |= 1ull << P.local_q[S.thr_pos[b]];
+            for (int i = 0; i < RB; i++)
+                if ((k >> i) & 1) g |= 1ull << P.local_q[S.reg_pos[i]];
+            return g;
+        };
+        const DevStage& Ld = plan.layouts[P.load_layout];
+        const DevStage& St = plan.layouts[P.store_layout];
+        for (int l = 0; l < PR_LANE_BITS; l++)
+            if (St.thr_pos[l] >= PR_LANE_BITS) return -5;     // store lanes must be the low positions
+        for (uint64_t tile = 0; tile < tiles; tile++) {
+            uint64_t base = 0;
+            for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
+            for (int t = 0; t < NT; t++)
+                for (int k = 0; k < NR; k++) regs[(size_t)t * NR + k] = sv[base | goff(Ld, t, k)];
+            // the layout the planner believes in, tracked through the swaps
+            int slot_pos[PR_TILE_BITS];
+            for (int l = 0; l < PR_LANE_BITS; l++) slot_pos[l] = Ld.thr_pos[l];
+            for (int r = 0; r < RB; r++) slot_pos[PR_LANE_BITS + r] = Ld.reg_pos[r];
+            for (int w = 0; w < 3; w++) slot_pos[PR_LANE_BITS + RB + w] = Ld.thr_pos[PR_LANE_BITS + w];
+            for (int o = P.op_begin; o < P.op_end; o++) {
+                const PairOp& op = plan.ops[o];
+                if (op.kind == PO_SWAP) {
+                    const int L = op.lane, R = op.reg;
+                    std::vector<double2> send((size_t)NT * NR);
+                    for (int t = 0; t < NT; t++) {
+                        const bool hi = (t >> L) & 1;
+                        for (int k = 0; k < NR; k++) {
+                            if (k & (1 << R)) continue;
+                            const int k1 = k | (1 << R);
+                            send[(size_t)t * NR + k] = hi ? regs[(size_t)t * NR + k] : regs[(size_t)t * NR + k1];
+                        }
+                    }
+                    for (int t = 0; t < NT; t++) {
+                        const bool hi = (t >> L) & 1;
+                        const int u = t ^ (1 << L);
+                        for (int k = 0; k < NR; k++) {
+                            if (k & (1 << R)) continue;
+                            const int k1 = k | (1 << R);
+                            const double2 recv = send[(size_t)u * NR + k];
+                            if (hi) regs[(size_t)t * NR + k] = recv;
+                            else regs[(size_t)t * NR + k1] = recv;
+                        }
+                    }
+                    std::swap(slot_pos[L], slot_pos[PR_LANE_BITS + R]);
+                } else if (op.kind == PO_RELAYOUT) {
+                    const DevStage& A = plan.layouts[op.src];
+                    const DevStage& B = plan.layouts[op.layout];
+                    for (int l = 0; l < PR_LANE_BITS; l++)
+                        if (A.thr_pos[l] != slot_pos[l]) return -2;
+                    for (int r = 0; r < RB; r++)
+                        if (A.reg_pos[r] != slot_pos[PR_LANE_BITS + r]) return -2;
+                    std::fill(written.begin(), written.end(), 0);
+                    for (int t = 0; t < NT; t++) {
+                        Slots s;
+                        make_slots<double, TB>(A, t, s);
+                        for (int k = 0; k < NR; k++) {
+                            const uint32_t sl = slot_of(s, k);
+                            if (sl >= 4096 || written[sl]++) return -3;
+                            sm[sl] = regs[(size_t)t * NR + k];
+                        }
+                    }
+                    for (int t = 0; t < NT; t++) {
+                        Slots s;
+                        make_slots<double, TB>(B, t, s);
+                        for (int k = 0; k < NR; k++) regs[(size_t)t * NR + k] = sm[slot_of(s, k)];
+                    }
+                    for (int l = 0; l < PR_LANE_BITS; l++) slot_pos[l] = B.thr_pos[l];
+                    for (int r = 0; r < RB; r++) slot_pos[PR_LANE_BITS + r] = B.reg_pos[r];
+                    for (int w = 0; w < 3; w++) slot_pos[PR_LANE_BITS + RB + w] = B.thr_pos[PR_LANE_BITS + w];
+                } else {
+                    int var = 0;
+                    for (int c = 0; c < op.ncond; c++) var |= (int)((base >> op.cond_q[c]) & 1ull) << c;
+                    const double* g = plan.gates.data() + (size_t)(op.gate + var) * 64;
+                    for (int w = 0; w < NT / 32; w++)
+                        for (int k = 0; k < NR; k++) {
+                            double D[8][8] = {{0}};
+                            for (int step = 0; step < 2; step++) {
+                                double A[8][4], Bm[4][8];
+                                for (int t = 0; t < 32; t++) {
+                                    const double2 x = regs[(size_t)(w * 32 + t) * NR + k];
+                                    A[t >> 2][t & 3] = step ? x.y : x.x;
+                                    Bm[t & 3][t >> 2] = g[2 * t + step];
+                                }
+                                for (int r = 0; r < 8; r++)
+                                    for (int c = 0; c < 8; c++) {
+                                        double acc = D[r][c];
+                                        for (int kk = 0; kk < 4; kk++) acc += A[r][kk] * Bm[kk][c];
+                                        D[r][c] = acc;
+                                    }
+                            }
+                            for (int t = 0; t < 32; t++)
+                                regs[(size_t)(w * 32 + t) * NR + k] =
+                                    make_double2(D[t >> 2][2 * (t & 3)], D[t >> 2][2 * (t & 3) + 1]);
+                        }
+                }
+            }
+            for (int l = 0; l < PR_LANE_BITS; l++)
+                if (St.thr_pos[l] != slot_pos[l]) return -4;
+            for (int r = 0; r < RB; r++)
+                if (St.reg_pos[r] != slot_pos[PR_LANE_BITS + r]) return -4;
+            for (int t = 0; t < NT; t++)
+                for (int k = 0; k < NR; k++) sv[base | goff(St, t, k)] = regs[(size_t)t * NR + k];
+        }
+    }
+    for (size_t i = 0; i < sv.size(); i++) {
+        re[i] = sv[i].x;
+        im[i] = sv[i].y;
+    }
+    if (stats) {
+        stats[0] = plan.passes.size();
+        stats[1] = plan.n_blocks;
+        stats[2] = plan.n_swaps;
+        stats[3] = plan.n_relayouts;
+    }
+    return 0;
+}
+
+// Plan statistics of the pair engine (no execution): passes, blocks, swaps, relayouts.
+extern "C" int emu_pairs_stats(uint32_t n, const svb_gate* gates, size_t n_gates, uint64_t* stats)
+{
+    std::vector<EOp> eops;
+    for (size_t i = 0; i < n_gates; i++)
+        if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
+    PairPlan plan;
+    if (!plan_pairs(eops, (int)n, plan)) return -6;
+    stats[0] = plan.passes.size();
+    stats[1] = plan.n_blocks;
+    stats[2] = plan.n_swaps;
+    stats[3] = plan.n_relayouts;
+    return 0;
+}

@@ -23,12 +23,13 @@ def z_terms(n):
 
 @pytest.mark.parametrize("n,prec,engine,k,tol", [
     (33, "fp64", "staged", 0, 1e-10),
+    (33, "fp64", "pairs", 0, 1e-10),
     (34, "fp32", "fused", 5, 2e-4),
 ])
 def test_round_trip_and_sampling(n, prec, engine, k, tol):
     from svsim_b200 import _native as nat
     P = nat.SVB_FP64 if prec == "fp64" else nat.SVB_FP32
-    E = nat.ENGINE_STAGED if engine == "staged" else nat.ENGINE_FUSED
+    E = {"staged": nat.ENGINE_STAGED, "pairs": nat.ENGINE_PAIRS, "fused": nat.ENGINE_FUSED}[engine]
     circ = circuits.random_matching_circuit(n, 20, seed=2024)
     h = nat.Handle(n, 0, P)
     try:

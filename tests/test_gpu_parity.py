@@ -316,3 +316,92 @@ def test_staged_equals_per_gate_at_n26():
     _, re1, im1 = run_gpu(n, g, nat.ENGINE_PER_GATE)
     _, re2, im2 = run_gpu(n, g, nat.ENGINE_STAGED, 12)
     assert np.max(np.abs(re1 - re2)) <= 1e-13 and np.max(np.abs(im1 - im2)) <= 1e-13
+
+
+# ---- pair engine (FP64 two-qubit blocks on the FP64 tensor cores) ---------------------
+
+def no_srn(g):
+    return g[g["op"] != G.OP["SRN"]]
+
+
+def test_pair_engine_brickwork_golden_and_samples():
+    """The 470-gate brickwork circuit at n=16 through the pair engine: amplitudes and
+    checksum against the reference's state and the 1024 samples of its own measure()."""
+    nat = native()
+    d = load_golden("brickwork.npz")
+    h, re, im = run_gpu(16, d["gates16"], nat.ENGINE_PAIRS)
+    assert h.plan_info().engine == nat.ENGINE_PAIRS
+    idx = d["idx16"]
+    assert np.max(np.abs(re[idx] - d["re16_at"])) <= FP64_TOL
+    assert np.max(np.abs(im[idx] - d["im16_at"])) <= FP64_TOL
+    i = np.arange(1 << 16, dtype=np.float64)
+    w = np.cos(0.7 * i) + 1j * np.sin(1.3 * i)
+    assert abs(np.sum((re + 1j * im) * w) - d["checksum16"][0]) <= 1e-10
+    samples, total = h.measure(d["uniforms16"])
+    assert np.array_equal(samples, d["samples16"])
+    assert abs(total - d["norm16"][0]) <= 1e-12
+
+
+@pytest.mark.parametrize("n", [12, 14, 17, 20, 22])
+def test_pair_engine_random_matching_vs_oracle(oracle, n):
+    nat = native()
+    g = circuits.random_matching_circuit(n, 8, seed=n + 1)
+    ore, oim = oracle.run(n, g)
+    _, re, im = run_gpu(n, g, nat.ENGINE_PAIRS)
+    assert_close(re, im, ore, oim)
+
+
+@pytest.mark.parametrize("n", [12, 15])
+def test_pair_engine_every_op_but_srn(oracle, n):
+    nat = native()
+    g = no_srn(mixed_circuit(n, 4, seed=n))
+    ore, oim = oracle.run(n, g)
+    _, re, im = run_gpu(n, g, nat.ENGINE_PAIRS)
+    assert_close(re, im, ore, oim)
+
+
+def test_pair_engine_from_arbitrary_state_and_qaoa(oracle):
+    nat = native()
+    n = 13
+    rng = np.random.default_rng(3)
+    st = (rng.standard_normal(1 << n), rng.standard_normal(1 << n))
+    g = no_srn(mixed_circuit(n, 2, seed=4))
+    ore, oim = oracle.run(n, g, state=st)
+    _, re, im = run_gpu(n, g, nat.ENGINE_PAIRS, state=st)
+    assert np.max(np.abs(re - ore)) <= 1e-11 and np.max(np.abs(im - oim)) <= 1e-11
+    q = circuits.qaoa_instances(1, n_min=16, n_max=16, seed=9)[0].circuit()
+    ore, oim = oracle.run(16, q)
+    _, re, im = run_gpu(16, q, nat.ENGINE_PAIRS)
+    assert_close(re, im, ore, oim)
+
+
+def test_pair_engine_matches_staged_on_device():
+    nat = native()
+    n = 26
+    g = circuits.random_matching_circuit(n, 12, seed=77)
+    ha = nat.Handle(n, 0, nat.SVB_FP64)
+    ha.set_engine(nat.ENGINE_PAIRS, 0, 0)
+    ha.set_circuit(g)
+    ha.run()
+    hb = nat.Handle(n, 0, nat.SVB_FP64)
+    hb.set_engine(nat.ENGINE_STAGED, 12, 0)
+    hb.set_circuit(g)
+    hb.run()
+    f, d = ha.compare(hb)
+    assert 1 - f <= 1e-12 and d <= 1e-13
+
+
+def test_pair_engine_rejects_srn_fp32_and_small_states():
+    nat = native()
+    h = nat.Handle(12, 0, nat.SVB_FP64)
+    h.set_engine(nat.ENGINE_PAIRS, 0, 0)
+    with pytest.raises(nat.SvbError) as e:
+        h.set_circuit(G.to_array([G.SRN(0)]))
+    assert e.value.status == nat.SVB_ERR_UNSUPPORTED
+    h11 = nat.Handle(11, 0, nat.SVB_FP64)
+    h11.set_engine(nat.ENGINE_PAIRS, 0, 0)
+    with pytest.raises(nat.SvbError):
+        h11.set_circuit(G.to_array([G.H(0)]))
+    h32 = nat.Handle(12, 0, nat.SVB_FP32)
+    with pytest.raises(nat.SvbError):
+        h32.set_engine(nat.ENGINE_PAIRS, 0, 0)

@@ -141,3 +141,43 @@ def test_fused_plan_rejects_srn(emu):
     g = G.to_array([G.H(0), G.SRN(3)])
     rc, *_ = run_fused_emu(emu, 12, g, 4)
     assert rc == -3
+
+
+def run_pairs_emu(lib, n, gates):
+    re = np.zeros(1 << n)
+    im = np.zeros(1 << n)
+    st = np.zeros(4, dtype=np.uint64)
+    vp = ctypes.c_void_p
+    rc = lib.emu_pairs_run(ctypes.c_uint32(n), vp(gates.ctypes.data), ctypes.c_size_t(len(gates)),
+                           vp(re.ctypes.data), vp(im.ctypes.data), vp(st.ctypes.data))
+    return rc, re, im, st
+
+
+@pytest.mark.parametrize("n,depth", [(12, 6), (13, 8), (16, 10), (17, 6)])
+def test_pair_plan_random_matching(emu, oracle, n, depth):
+    """Pair-engine plan (two-qubit blocks, lane/register exchanges, relayouts, tile-
+    selected variants) run thread by thread with the kernel's data movement and MMA
+    fragment rules, against the oracle."""
+    g = circuits.random_matching_circuit(n, depth, seed=n + depth)
+    rc, re, im, st = run_pairs_emu(emu, n, g)
+    assert rc == 0, rc
+    ore, oim = oracle.run(n, g)
+    assert np.max(np.abs((re + 1j * im) - (ore + 1j * oim))) < 1e-13
+    assert st[1] <= len(g)                  # no more blocks than gates
+
+
+def test_pair_plan_every_op_but_srn_and_qaoa(emu, oracle):
+    for n, g in [(15, mixed_circuit(15, 3, seed=31)),
+                 (14, circuits.qaoa_instances(1, n_min=14, n_max=14, seed=5)[0].circuit()),
+                 (16, circuits.brickwork_circuit(16, 20))]:
+        g = g[g["op"] != G.OP["SRN"]]
+        rc, re, im, _ = run_pairs_emu(emu, n, g)
+        assert rc == 0, rc
+        ore, oim = oracle.run(n, g)
+        assert np.max(np.abs((re + 1j * im) - (ore + 1j * oim))) < 1e-13
+
+
+def test_pair_plan_rejects_srn_and_small_states(emu):
+    g = G.to_array([G.H(0), G.SRN(1)])
+    assert run_pairs_emu(emu, 12, g)[0] == -6
+    assert run_pairs_emu(emu, 11, G.to_array([G.H(0)]))[0] == -6
