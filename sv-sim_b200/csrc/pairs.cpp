@@ -491,6 +491,7 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan)
                     busy |= m;
                     if (c == 0) break;
                 }
+                if (best < 0) best = (int)first;     // the first open block is always ready
                 done[best] = 1;
                 order.push_back(best);
                 // advance the probe layout as the real planner will (next use in
