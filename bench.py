@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--tile-bits", type=int, default=12)
     ap.add_argument("--engine", choices=["staged", "pairs"], default="pairs",
                     help="FP64 engine of the headline step")
-    ap.add_argument("--form", choices=["headline", "pergate", "fused", "qaoa", "capacity"], default="headline",
+    ap.add_argument("--form", choices=["headline", "pergate", "fused", "qaoa", "capacity", "adjoint"],
+                    default="headline",
                     help="headline: the FP64 n=30 step (the measured line); the others run one "
                          "secondary form alone (for profiling and capacity runs)")
     ap.add_argument("--instances", type=int, default=512, help="QAOA batch size (--form qaoa)")
@@ -491,7 +492,9 @@ def run_form(args):
     if rank != 0:
         return
     torch.cuda.set_device(local)
-    if args.form == "pergate":
+    if args.form == "adjoint":
+        res = adjoint_form(local)
+    elif args.form == "pergate":
         from svsim_b200 import circuits
         res = per_gate_form(local, circuits.random_matching_circuit(args.qubits, DEPTH, seed=SEED), n=args.qubits)
     elif args.form == "fused":
@@ -533,27 +536,18 @@ def per_gate_form(device, circuit, n=N_QUBITS):
             "kernels": "k_eop_pairs / k_cx (4 pairs per thread in flight)"}
 
 
-def secondary_forms(device, circuit):
-    """Per-gate FP64 sweeps on the same circuit, and adjoint gradients (n=20, 480 params)."""
-    import torch
+def adjoint_form(device, reps=5):
+    """Adjoint gradients of the n=20, 480-parameter ansatz against parameter shift on the
+    same GPU (2 circuits per parameter, timed on 48 of 480 and scaled)."""
     from svsim_b200 import circuits, _native as nat
-    forms = {}
-    forms["per_gate_fp64"] = per_gate_form(device, circuit)
-    forms["fused_tc_fp32"] = fused_form(device, circuit)
-    forms["qaoa_batch_fp64"] = qaoa_form(device, 512, "fp64")
-    forms["qaoa_batch_fp32"] = qaoa_form(device, 512, "fp32")
-    forms["capacity"] = capacity_form(device)
-    # adjoint: n=20 hardware-efficient ansatz, 720 gates, 480 parameters
     pc = circuits.hardware_efficient_ansatz()
     terms = circuits.zz_x_hamiltonian(20)
     ha = nat.Handle(20, device, nat.SVB_FP64)
     ha.adjoint(pc.gates, pc.binding, 480, terms)
-    reps = 5
     t0 = time.perf_counter()
     for _ in range(reps):
         ha.adjoint(pc.gates, pc.binding, 480, terms)
     t_adj = (time.perf_counter() - t0) / reps
-    # parameter shift on the same GPU: 2 circuits per parameter (timed on 48 of 480)
     hp = nat.Handle(20, device, nat.SVB_FP64)
     nshift = 48
     t0 = time.perf_counter()
@@ -566,11 +560,23 @@ def secondary_forms(device, circuit):
             hp.run()
             hp.expectation(terms)
     t_shift = (time.perf_counter() - t0) / nshift * 480
-    forms["adjoint"] = {"grads_per_s": 1.0 / t_adj, "param_shift_grads_per_s": 1.0 / t_shift,
-                        "speedup_vs_param_shift": t_shift / t_adj,
-                        "workload": "n=20, 12 layers RY+RZ+CX ring, 720 gates, P=480, "
-                                    "H = sum ZZ + 0.5 sum X",
-                        "param_shift_sample": f"{nshift} of 480 parameters timed, scaled"}
+    return {"grads_per_s": 1.0 / t_adj, "param_shift_grads_per_s": 1.0 / t_shift,
+            "speedup_vs_param_shift": t_shift / t_adj,
+            "workload": "n=20, 12 layers RY+RZ+CX ring, 720 gates, P=480, H = sum ZZ + 0.5 sum X",
+            "param_shift_sample": f"{nshift} of 480 parameters timed, scaled"}
+
+
+def secondary_forms(device, circuit):
+    """Per-gate FP64 sweeps on the same circuit, and adjoint gradients (n=20, 480 params)."""
+    import torch
+    from svsim_b200 import circuits, _native as nat
+    forms = {}
+    forms["per_gate_fp64"] = per_gate_form(device, circuit)
+    forms["fused_tc_fp32"] = fused_form(device, circuit)
+    forms["qaoa_batch_fp64"] = qaoa_form(device, 512, "fp64")
+    forms["qaoa_batch_fp32"] = qaoa_form(device, 512, "fp32")
+    forms["capacity"] = capacity_form(device)
+    forms["adjoint"] = adjoint_form(device)
     return forms
 
 

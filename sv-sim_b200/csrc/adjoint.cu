@@ -331,46 +331,47 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
     }
 
     cudaError_t err = cudaSuccess;
-    double2* lam = nullptr;
-    double* partial = nullptr;
-    double* results = nullptr;
-    svb_pauli_term* dterms = nullptr;
-    std::vector<void*> ckpts;
-    std::vector<size_t> ckpt_at;   // op index where checkpoint c was taken (state before op)
-    auto cleanup = [&]() {
-        cudaFree(lam); cudaFree(partial); cudaFree(results); cudaFree(dterms);
-        for (void* p : ckpts) cudaFree(p);
-        lam = nullptr; partial = nullptr; results = nullptr; dterms = nullptr;
-        ckpts.clear();
-    };
+    AdjScratch& A = s->adj;
+    const size_t sbytes = dim * sizeof(double2);
+    // buffers live in the handle and are reused by later calls; large states give them
+    // back at the end of the call
+    const bool keep = sbytes <= (size_t(256) << 20);
     auto fail = [&](cudaError_t e, const char* what) {
-        cleanup();
+        if (!keep) free_adjoint_scratch(A);
         set_error(std::string("svb_adjoint: ") + what + ": " + cudaGetErrorString(e));
         (void)cudaGetLastError();
         return e == cudaErrorMemoryAllocation ? SVB_ERR_OOM : SVB_ERR_CUDA;
     };
-    const size_t sbytes = dim * sizeof(double2);
-    if ((err = cudaMalloc(&lam, sbytes)) != cudaSuccess) return fail(err, "cudaMalloc(lambda)");
     const size_t nslots = std::max<size_t>(slots.size(), 1);
-    if ((err = cudaMalloc(&partial, (nslots + 1) * ADJ_BLOCKS * sizeof(double))) != cudaSuccess)
+    if ((err = grow(A.lam, sbytes)) != cudaSuccess) return fail(err, "cudaMalloc(lambda)");
+    if ((err = grow(A.partial, (nslots + 1) * ADJ_BLOCKS * sizeof(double))) != cudaSuccess)
         return fail(err, "cudaMalloc(partials)");
-    if ((err = cudaMalloc(&results, (nslots + 1) * sizeof(double))) != cudaSuccess)
+    if ((err = grow(A.results, (nslots + 1) * sizeof(double))) != cudaSuccess)
         return fail(err, "cudaMalloc(results)");
-    if (n_terms && (err = cudaMalloc(&dterms, n_terms * sizeof(svb_pauli_term))) != cudaSuccess)
+    if ((err = grow(A.terms, std::max<size_t>(1, n_terms) * sizeof(svb_pauli_term))) != cudaSuccess)
         return fail(err, "cudaMalloc(terms)");
+    if ((err = grow(A.final_state, sbytes)) != cudaSuccess) return fail(err, "cudaMalloc(final state)");
+    double2* lam = static_cast<double2*>(A.lam.p);
+    double* partial = static_cast<double*>(A.partial.p);
+    double* results = static_cast<double*>(A.results.p);
+    svb_pauli_term* dterms = static_cast<svb_pauli_term*>(A.terms.p);
     if (n_terms && (err = cudaMemcpy(dterms, terms, n_terms * sizeof(svb_pauli_term),
                                      cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(err, "terms upload");
 
     // checkpoints: up to 4 evenly spaced, if they fit in a quarter of free memory
+    std::vector<void*> ckpts;
+    std::vector<size_t> ckpt_at;   // op index where checkpoint c was taken (state before op)
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    int n_ck = (int)std::min<size_t>(4, free_b / 4 / sbytes);
+    size_t held = 0;
+    for (const GrowBuf& b : A.ckpts) held += b.cap >= sbytes ? sbytes : 0;
+    int n_ck = (int)std::min<size_t>(4, (free_b + held) / 4 / sbytes);
     if (K < 64) n_ck = 0;
+    if ((int)A.ckpts.size() < n_ck) A.ckpts.resize(n_ck);
     for (int c = 0; c < n_ck; c++) {
-        void* p = nullptr;
-        if ((err = cudaMalloc(&p, sbytes)) != cudaSuccess) { (void)cudaGetLastError(); break; }
-        ckpts.push_back(p);
+        if ((err = grow(A.ckpts[c], sbytes)) != cudaSuccess) { (void)cudaGetLastError(); break; }
+        ckpts.push_back(A.ckpts[c].p);
         ckpt_at.push_back(K * (size_t)(c + 1) / (size_t)(n_ck + 1));
     }
 
@@ -380,13 +381,19 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
     for (size_t c = 0; c <= ckpts.size(); c++) {
         const size_t end = c < ckpts.size() ? ckpt_at[c] : K;
         std::vector<EOp> seg(eops.begin() + begin, eops.begin() + end);
-        svb_status r2 = run_eops_staged(n, s->state, seg, nullptr);
-        if (r2 != SVB_OK) { cleanup(); return r2; }
+        svb_status r2 = run_eops_staged(n, s->state, seg, nullptr, A);
+        if (r2 != SVB_OK) {
+            if (!keep) free_adjoint_scratch(A);
+            return r2;
+        }
         if (c < ckpts.size() &&
             (err = cudaMemcpyAsync(ckpts[c], s->state, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
             return fail(err, "checkpoint");
         begin = end;
     }
+    // psi(p), handed back in the handle at the end
+    if ((err = cudaMemcpyAsync(A.final_state.p, s->state, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
+        return fail(err, "final state copy");
     // lambda = H psi, energy = Re <psi|lambda>
     const unsigned g = adj_grid(dim);
     if (n_terms)
@@ -443,8 +450,9 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
             if (b.idx[f] >= 0 && e.jac[slots[r].i][f] != 0.0)
                 grad[b.idx[f]] += 2.0 * host[r] * e.jac[slots[r].i][f] * b.coef[f];
     }
-    // leave psi(p) in the handle: rerun the forward plan
-    cleanup();
-    if ((err = launch_reset<double>(s->state, n, nullptr)) != cudaSuccess) return fail(err, "reset");
-    return svb_run(s, nullptr);
+    // leave psi(p) in the handle
+    if ((err = cudaMemcpy(s->state, A.final_state.p, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
+        return fail(err, "final state restore");
+    if (!keep) free_adjoint_scratch(A);
+    return SVB_OK;
 }

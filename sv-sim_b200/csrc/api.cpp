@@ -86,6 +86,7 @@ void free_plan(Sim* s)
 
 void free_scratch(Sim* s)
 {
+    free_adjoint_scratch(s->adj);
     cudaFree(s->mscr.block_sums);
     cudaFree(s->mscr.block_prefix);
     cudaFree(s->mscr.uniforms);
@@ -196,7 +197,39 @@ bool use_graph(const Sim* s)
 
 }  // namespace
 
-svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st)
+cudaError_t grow(GrowBuf& b, size_t bytes)
+{
+    if (b.cap >= bytes && b.p) return cudaSuccess;
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    const cudaError_t e = cudaMalloc(&b.p, std::max<size_t>(bytes, 16));
+    if (e == cudaSuccess) b.cap = std::max<size_t>(bytes, 16);
+    else b.p = nullptr;
+    return e;
+}
+
+void release(GrowBuf& b)
+{
+    cudaFree(b.p);
+    b = GrowBuf{};
+}
+
+void free_adjoint_scratch(AdjScratch& a)
+{
+    release(a.lam);
+    release(a.partial);
+    release(a.results);
+    release(a.terms);
+    release(a.final_state);
+    release(a.plan_passes);
+    release(a.plan_stages);
+    release(a.plan_ops);
+    for (GrowBuf& b : a.ckpts) release(b);
+    a.ckpts.clear();
+}
+
+svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st, AdjScratch& cache)
 {
     const int M = n >= 20 ? 12 : (n >= 12 ? 10 : n);
     if (M < 10) {
@@ -209,10 +242,15 @@ svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cuda
     StagedPlan P;
     plan_staged(ops, n, M, 3, P);
     if (P.passes.empty()) return SVB_OK;
+    // the previous segment's kernels may still read the plan buffers: wait before reuse
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = grow(cache.plan_passes, P.passes.size() * sizeof(DevPass));
+    if (e == cudaSuccess) e = grow(cache.plan_stages, std::max<size_t>(1, P.stages.size()) * sizeof(DevStage));
+    if (e == cudaSuccess) e = grow(cache.plan_ops, std::max<size_t>(1, P.ops.size()) * sizeof(DevOp));
     DevPlanBuffers b;
-    cudaError_t e = cudaMalloc(&b.passes, P.passes.size() * sizeof(DevPass));
-    if (e == cudaSuccess) e = cudaMalloc(&b.stages, std::max<size_t>(1, P.stages.size()) * sizeof(DevStage));
-    if (e == cudaSuccess) e = cudaMalloc(&b.ops, std::max<size_t>(1, P.ops.size()) * sizeof(DevOp));
+    b.passes = static_cast<DevPass*>(cache.plan_passes.p);
+    b.stages = static_cast<DevStage*>(cache.plan_stages.p);
+    b.ops = static_cast<DevOp*>(cache.plan_ops.p);
     if (e == cudaSuccess)
         e = cudaMemcpy(b.passes, P.passes.data(), P.passes.size() * sizeof(DevPass), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !P.stages.empty())
@@ -221,10 +259,6 @@ svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cuda
         e = cudaMemcpy(b.ops, P.ops.data(), P.ops.size() * sizeof(DevOp), cudaMemcpyHostToDevice);
     for (size_t p = 0; e == cudaSuccess && p < P.passes.size(); p++)
         e = launch_staged_pass<double>(state, n, M, (int)p, b, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(b.passes);
-    cudaFree(b.stages);
-    cudaFree(b.ops);
     if (e != cudaSuccess) return cuda_fail(e, "staged run");
     return SVB_OK;
 }

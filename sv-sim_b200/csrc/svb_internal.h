@@ -299,9 +299,26 @@ cudaError_t compare_device(const void* a, const void* b, int n, double* d_out5, 
 // ---------------------------------------------------------------------------------
 // Adjoint (adjoint.cu)
 // ---------------------------------------------------------------------------------
+// A device buffer kept by the handle and reallocated only when a call needs more.
+struct GrowBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+cudaError_t grow(GrowBuf& b, size_t bytes);
+void release(GrowBuf& b);
+
+// Scratch of svb_adjoint, reused across calls on the same handle.
+struct AdjScratch {
+    GrowBuf lam, partial, results, terms, final_state;
+    GrowBuf plan_passes, plan_stages, plan_ops;     // forward segments' staged plans
+    std::vector<GrowBuf> ckpts;
+};
+
 // Runs elementary ops on an FP64 device state with the staged engine (per-gate for
-// n < 10); synchronous.
-svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st);
+// n < 10), queued on `st`.  The plan is uploaded into `cache`'s buffers.
+svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st,
+                           AdjScratch& cache);
+void free_adjoint_scratch(AdjScratch& a);
 
 // ---------------------------------------------------------------------------------
 // The handle
@@ -330,6 +347,7 @@ struct Sim {
     // scratch
     MeasureScratch mscr;
     double* d_small = nullptr;     // a few doubles for reduction results
+    AdjScratch adj;
 };
 
 void set_error(const std::string& msg);
