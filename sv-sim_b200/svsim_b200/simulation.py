@@ -44,6 +44,21 @@ class Simulation:
         self.circuit: list[_g.Gate] = []
         self._uploaded = False
 
+    @classmethod
+    def from_qasm(cls, source: str, i_gpu: int = 0, precision: str = "fp64",
+                  engine: int = ENGINE_AUTO, tile_bits: int = 0) -> "Simulation":
+        """A Simulation holding an OpenQASM 2.0 program (a file path or the program text),
+        with one qubit per declared qubit (registers in declaration order).  The
+        program's measure records are kept in ``qasm_measured``."""
+        import os
+        from . import qasm
+        prog = qasm.load(source) if os.path.isfile(source) else qasm.loads(source)
+        sim = cls(prog.n_qubits, i_gpu, precision, engine, tile_bits)
+        for g in _g.from_array(prog.gates):
+            sim.append(g)
+        sim.qasm_measured = prog.measured
+        return sim
+
     # ---- circuit ----------------------------------------------------------------------
     @property
     def n_gates(self) -> int:
