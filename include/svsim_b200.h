@@ -191,6 +191,23 @@ svb_status svb_expectation(svb_sim* sim, const svb_pauli_term* terms, size_t n_t
  * accuracy report of the FP32 engines against FP64; no reference counterpart). */
 svb_status svb_compare_states(svb_sim* a, svb_sim* b, double* fidelity, double* max_abs_diff);
 
+/* ---- immediate-mode operations of the Q#/QIR variant ---------------------------- */
+
+/* Replaces the masked multi-controlled gates of svsim_qsharp/svsim_nvgpu_sin.cuh
+ * (ControlledX ... ControlledAdjointT, OP_HEAD_MASK :680-690): applies the 2x2 complex
+ * matrix m (row-major, re/im interleaved: m00r m00i m01r m01i m10r m10i m11r m11i) to
+ * `target` on the amplitudes whose control_mask bits are all 1, at once on `stream`
+ * (not part of the circuit).  The target may not be in the mask. */
+svb_status svb_apply_controlled(svb_sim* sim, uint32_t target, uint64_t control_mask, const double* m,
+                                void* stream);
+
+/* Replaces Measure_GATE of the Q# variant (:1486-1600): measures `qubit` in the Pauli
+ * basis `pauli` (0 = Z, 1 = X, 2 = Y) and collapses the state on the GPU.  The outcome is
+ * 1 when the caller's uniform r < P(1) (P(1) summed in FP64); the other half is zeroed
+ * and the kept half scaled by 1/sqrt(P(outcome)).  Writes the outcome and P(1). */
+svb_status svb_measure_qubit(svb_sim* sim, uint32_t qubit, int pauli, double r, int* outcome,
+                             double* prob_one);
+
 /* ---- differentiation (no reference counterpart) --------------------------------- */
 
 /* Adjoint differentiation of E(p) = <psi(p)| H |psi(p)>, psi(p) = U(p)|0..0>:

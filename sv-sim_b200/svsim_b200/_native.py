@@ -74,6 +74,9 @@ _SIGS = {
     "svb_qaoa_launch": ([_vp, _vp], ctypes.c_int),
     "svb_qaoa_info": ([_vp, ctypes.POINTER(QaoaStats)], ctypes.c_int),
     "svb_qaoa_destroy": ([_vp], ctypes.c_int),
+    "svb_apply_controlled": ([_vp, ctypes.c_uint32, ctypes.c_uint64, _dp, _vp], ctypes.c_int),
+    "svb_measure_qubit": ([_vp, ctypes.c_uint32, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_int),
+                           _dp], ctypes.c_int),
     "svb_last_error": ([], ctypes.c_char_p),
     "svb_version": ([], ctypes.c_char_p),
 }
@@ -193,6 +196,24 @@ class Handle:
         d = ctypes.c_double()
         check(lib().svb_compare_states(self.ptr, other.ptr, ctypes.byref(f), ctypes.byref(d)))
         return f.value, d.value
+
+    def apply_controlled(self, target: int, controls, matrix, stream: int = 0):
+        """Applies the complex 2x2 `matrix` to `target` where every qubit in `controls`
+        is 1 (the Q# variant's masked controlled gates)."""
+        mask = 0
+        for c in controls:
+            mask |= 1 << int(c)
+        u = np.asarray(matrix, dtype=np.complex128).reshape(2, 2)
+        m = np.array([u[0, 0].real, u[0, 0].imag, u[0, 1].real, u[0, 1].imag,
+                      u[1, 0].real, u[1, 0].imag, u[1, 1].real, u[1, 1].imag])
+        check(lib().svb_apply_controlled(self.ptr, target, mask, dptr(m), _vp(stream)))
+
+    def measure_qubit(self, qubit: int, r: float, pauli: int = 0):
+        """Mid-circuit measurement with collapse: returns (outcome, P(1))."""
+        out = ctypes.c_int()
+        p1 = ctypes.c_double()
+        check(lib().svb_measure_qubit(self.ptr, qubit, pauli, float(r), ctypes.byref(out), ctypes.byref(p1)))
+        return out.value, p1.value
 
     def adjoint(self, gates, bindings, n_params, terms):
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)

@@ -17,11 +17,11 @@ def program_text(n, depth, seed):
     regs = [f"lo[{k}]" for k in range(n // 2)] + [f"hi[{k}]" for k in range(n - n // 2)]
     for _ in range(depth):
         for q in regs:
-            a = rng.uniform(0, 2 * np.pi, size=3)
+            a = [float(x) for x in rng.uniform(0, 2 * np.pi, size=3)]
             lines.append(f"u3({a[0]!r}, {a[1]!r}, {a[2]!r}) {q};")
         perm = rng.permutation(n)
         for i in range(n // 2):
-            lines.append(f"ent({rng.uniform(-1, 1)!r}*pi) {regs[perm[2 * i]]}, {regs[perm[2 * i + 1]]};")
+            lines.append(f"ent({float(rng.uniform(-1, 1))!r}*pi) {regs[perm[2 * i]]}, {regs[perm[2 * i + 1]]};")
     lines.append("measure lo[0] -> c[0];")
     return "\n".join(lines)
 
