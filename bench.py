@@ -260,7 +260,8 @@ def run_ours(args):
     achieved = per_launch_bytes / launch_s / 1e9
     peak, peak_kind = peaks()
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "staged_fp64_traffic.txt")
+    tfile = os.path.join(ROOT, "profiles", "pairs_fp64_traffic.txt" if args.engine == "pairs"
+                         else "staged_fp64_traffic.txt")
     if os.path.exists(tfile):
         for ln in open(tfile):
             if ln.startswith("bytes_per_launch_n30"):
@@ -409,13 +410,13 @@ def qaoa_form(device, count=512, precision="fp64", reps=5):
 
 
 def capacity_form(device, shots=4096):
-    """The largest states of one B200: n=33 FP64 (staged, 128 GiB) and n=34 FP32 (fused,
+    """The largest states of one B200: n=33 FP64 (pair engine, 128 GiB) and n=34 FP32 (fused,
     128 GiB), depth-20 random-matching circuits, 4096-shot sampling with the FP64 CDF."""
     import torch
     from svsim_b200 import circuits, _native as nat
     out = {}
     uni = np.random.default_rng(1).random(shots)
-    for n, prec, eng, k, name in ((33, nat.SVB_FP64, nat.ENGINE_STAGED, 0, "n33_fp64_staged"),
+    for n, prec, eng, k, name in ((33, nat.SVB_FP64, nat.ENGINE_PAIRS, 0, "n33_fp64_pairs"),
                                   (34, nat.SVB_FP32, nat.ENGINE_FUSED, 5, "n34_fp32_fused")):
         circ = circuits.random_matching_circuit(n, 20, seed=SEED)
         h = nat.Handle(n, device, prec)

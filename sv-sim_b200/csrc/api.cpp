@@ -393,8 +393,12 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
     int engine = s->engine_req;
     const int n = (int)s->n;
     const int M = pick_tile_bits(s);
-    if (engine == SVB_ENGINE_AUTO)
-        engine = (staged_supported(s->precision, M) && n >= M) ? SVB_ENGINE_STAGED : SVB_ENGINE_PER_GATE;
+    if (engine == SVB_ENGINE_AUTO) {
+        // FP64 circuits of >= 12 qubits go to the pair engine (FP64 tensor cores) unless they
+        // hold SRN, which has no matrix; otherwise the staged engine, per-gate below its tile
+        if (s->precision == SVB_FP64 && n >= PR_TILE_BITS && fusable(s->eops)) engine = SVB_ENGINE_PAIRS;
+        else engine = (staged_supported(s->precision, M) && n >= M) ? SVB_ENGINE_STAGED : SVB_ENGINE_PER_GATE;
+    }
     if (engine == SVB_ENGINE_FUSED) {
         if (s->precision != SVB_FP32 || n < FT_TILE_BITS) {
             set_error("svb_set_circuit: the fused engine needs an FP32 state of >= 12 qubits");
