@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--tile-bits", type=int, default=12)
     ap.add_argument("--engine", choices=["staged", "pairs"], default="pairs",
                     help="FP64 engine of the headline step")
-    ap.add_argument("--form", choices=["headline", "pergate", "fused", "qaoa", "capacity", "adjoint"],
+    ap.add_argument("--form", choices=["headline", "pergate", "fused", "qaoa", "capacity", "adjoint", "density"],
                     default="headline",
                     help="headline: the FP64 n=30 step (the measured line); the others run one "
                          "secondary form alone (for profiling and capacity runs)")
@@ -495,6 +495,8 @@ def run_form(args):
     torch.cuda.set_device(local)
     if args.form == "adjoint":
         res = adjoint_form(local)
+    elif args.form == "density":
+        res = density_form(local)
     elif args.form == "pergate":
         from svsim_b200 import circuits
         res = per_gate_form(local, circuits.random_matching_circuit(args.qubits, DEPTH, seed=SEED), n=args.qubits)
@@ -535,6 +537,39 @@ def per_gate_form(device, circuit, n=N_QUBITS):
             "frac_of_peak": info.moved_bytes / s / 1e9 / peak,
             "sample": "first 4 layers (180 gates), one sweep per gate (CX: half sweep)",
             "kernels": "k_eop_pairs / k_cx (4 pairs per thread in flight)"}
+
+
+def density_form(device, n=14, depth=10, reps=3):
+    """Density matrix of n=14 qubits (a 28-qubit FP64 vector, 4 GiB) through a depth-10
+    random-matching circuit with a depolarizing channel (p = 0.01) after every gate on each
+    qubit it touches; superoperator blocks on the pair engine."""
+    import torch
+    from svsim_b200 import circuits, density as D
+    g = circuits.random_matching_circuit(n, depth, seed=SEED)
+    dm = D.DensityMatrix(n, device)
+    dm.set_circuit(g, D.depolarizing(0.01))
+    info = dm.plan_info()
+    dm.run()
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        dm.handle.run()
+    e1.record()
+    torch.cuda.synchronize(device)
+    sec = e0.elapsed_time(e1) / 1e3 / reps
+    dm.reset()                                       # one fresh run for the trace and purity
+    dm.run()
+    p = dm.probabilities()
+    peak, _ = peaks()
+    out = {"gates_per_s": len(g) / sec, "ms_per_circuit": sec * 1e3, "passes": int(info.n_passes),
+           "engine": int(info.engine), "hbm_gbs": info.moved_bytes / sec / 1e9,
+           "frac_of_peak": info.moved_bytes / sec / 1e9 / peak, "trace": float(p.sum()),
+           "purity": dm.handle.norm2(),
+           "workload": f"rho of n={n} (2n={2 * n} vector qubits), depth {depth}, depolarizing 0.01"}
+    dm.close()
+    torch.cuda.empty_cache()
+    return out
 
 
 def adjoint_form(device, reps=5):
@@ -578,6 +613,7 @@ def secondary_forms(device, circuit):
     forms["qaoa_batch_fp32"] = qaoa_form(device, 512, "fp32")
     forms["capacity"] = capacity_form(device)
     forms["adjoint"] = adjoint_form(device)
+    forms["density_matrix"] = density_form(device)
     return forms
 
 

@@ -209,6 +209,25 @@ svb_status svb_apply_controlled(svb_sim* sim, uint32_t target, uint64_t control_
 svb_status svb_measure_qubit(svb_sim* sim, uint32_t qubit, int pauli, double r, int* outcome,
                              double* prob_one);
 
+/* ---- density matrices with noise (the reference's svsim_qsharp_noise variant) ----- */
+
+/* A density-matrix handle for rho of n_qubits qubits (1..17): an FP64 state of 2 n_qubits
+ * qubits holding rho[i][j] at index i + 2^n j (the noise variant's layout, dim 2^(2n) at
+ * svsim_qsharp_noise/svsim_nvgpu_sin.cuh:527-529), set to |0..0><0..0|.  svb_run,
+ * svb_reset_state and svb_destroy apply to it; svb_norm2 gives Tr(rho^2). */
+svb_status svb_dm_create(uint32_t n_qubits, int device, svb_sim** out);
+
+/* The circuit of a density-matrix handle: every gate U becomes rho -> U rho U^dagger, and
+ * when n_kraus > 0 the one-qubit channel with Kraus operators noise_kraus (n_kraus 2x2
+ * complex matrices, row-major, re/im interleaved: 8 doubles each) is applied after every
+ * gate to each qubit the gate touches (the variant's noisy gates, a superoperator per
+ * gate).  SRN has no superoperator and is rejected. */
+svb_status svb_dm_set_circuit(svb_sim* sim, const svb_gate* gates, size_t n_gates,
+                              const double* noise_kraus, uint32_t n_kraus);
+
+/* The diagonal of rho (the outcome probabilities), 2^n_qubits doubles, to the host. */
+svb_status svb_dm_probabilities(svb_sim* sim, double* out);
+
 /* ---- differentiation (no reference counterpart) --------------------------------- */
 
 /* Adjoint differentiation of E(p) = <psi(p)| H |psi(p)>, psi(p) = U(p)|0..0>:

@@ -180,6 +180,7 @@ svb_status launch_all(Sim* s, cudaStream_t st)
         for (const EOp& op : s->eops) {
             cudaError_t e = dispatch_prec(s->precision, [&](auto t) {
                 using T = decltype(t);
+                if (op.form == F_M4) return launch_m4<T>(s->state, n, (int)op.q, (int)op.c, s->mats[op.mat], st);
                 return launch_eop<T>(s->state, n, op, st);
             });
             if (e != cudaSuccess) return cuda_fail(e, "gate launch");
@@ -196,6 +197,8 @@ bool use_graph(const Sim* s)
 }
 
 }  // namespace
+
+int gate_qubit_slots(uint32_t op) { return n_qubit_slots(op); }
 
 cudaError_t grow(GrowBuf& b, size_t bytes)
 {
@@ -386,13 +389,38 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
         lower_gate(gates[i], (int32_t)i, eops);
         sweeps += reference_sweeps(gates[i].op);
     }
+    s->mats.clear();
+    return set_circuit_lowered(s, eops, gates, n_gates, sweeps);
+}
+
+}  // extern "C"
+
+namespace svb {
+
+svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* gates, size_t n_gates, double sweeps)
+{
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    bool has_m4 = false;
+    for (const EOp& e : eops) has_m4 |= e.form == F_M4;
+    std::vector<Mat4> mats;
+    mats.swap(s->mats);                    // free_plan leaves them alone; keep them with the plan
     free_plan(s);
-    s->gates.assign(gates, gates + n_gates);
+    s->mats.swap(mats);
+    if (gates) s->gates.assign(gates, gates + n_gates);
     s->eops.swap(eops);
 
     int engine = s->engine_req;
     const int n = (int)s->n;
     const int M = pick_tile_bits(s);
+    if (has_m4) {
+        // general 4x4 blocks: the pair engine, or per-gate sweeps below its tile
+        if (engine == SVB_ENGINE_AUTO)
+            engine = (s->precision == SVB_FP64 && n >= PR_TILE_BITS) ? SVB_ENGINE_PAIRS : SVB_ENGINE_PER_GATE;
+        if (engine != SVB_ENGINE_PAIRS && engine != SVB_ENGINE_PER_GATE) {
+            set_error("svb_set_circuit: two-qubit matrix blocks run on the pair or the per-gate engine");
+            return SVB_ERR_UNSUPPORTED;
+        }
+    }
     if (engine == SVB_ENGINE_AUTO) {
         // FP64 circuits of >= 12 qubits go to the pair engine (FP64 tensor cores) unless they
         // hold SRN, which has no matrix; otherwise the staged engine, per-gate below its tile
@@ -461,7 +489,7 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
         // one read + write per pass, then the renormalisation (two reads, one write)
         s->info.moved_bytes = 2.0 * sb * (double)F.passes.size() + (F.passes.empty() ? 0.0 : 3.0 * sb);
     } else if (engine == SVB_ENGINE_PAIRS) {
-        if (!plan_pairs(s->eops, n, s->pairs)) {
+        if (!plan_pairs(s->eops, n, s->pairs, &s->mats)) {
             set_error("svb_set_circuit: the pair planner rejected the circuit");
             return SVB_ERR_UNSUPPORTED;
         }
@@ -520,11 +548,16 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
         double moved = 0;
         for (const EOp& e : s->eops)
             moved += (e.form == F_CX) ? 0.5 * sb : (form_is_diag(e.form) && e.form != F_DIAG) ? sb : 2.0 * sb;
+        // (F_M4 blocks count as dense: one read and one write)
         s->info.moved_bytes = moved;
     }
     s->have_circuit = true;
     return SVB_OK;
 }
+
+}  // namespace svb
+
+extern "C" {
 
 svb_status svb_clear_circuit(svb_sim* s)
 {

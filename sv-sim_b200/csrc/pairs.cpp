@@ -227,6 +227,12 @@ struct PassPairs {
         ph.v = nv;
         ph.active = true;
     }
+    // a general two-qubit matrix on (a: bit 0, b: bit 1)
+    void add_m4(int a, int b, const M4& m)
+    {
+        if (cond_union(pend[a].cond, pend[b].cond).size() > (size_t)PR_MAX_COND) flush(a);
+        close(a, b, &m);
+    }
     void add_cx(int c, int t)
     {
         if (cond_union(pend[c].cond, pend[t].cond).size() > (size_t)PR_MAX_COND) flush(c);
@@ -414,12 +420,14 @@ void write_block(PairPlan& plan, const Block& b, bool transposed)
 
 }  // namespace
 
-bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan)
+bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::vector<Mat4>* mats)
 {
     plan = PairPlan{};
     if (n < PR_TILE_BITS) return false;
-    for (const EOp& e : ops)
+    for (const EOp& e : ops) {
         if (e.form == F_SRN) return false;      // only real-linear: not a matrix
+        if (e.form == F_M4 && (!mats || e.mat < 0 || (size_t)e.mat >= mats->size())) return false;
+    }
     select_passes(ops, n, PR_TILE_BITS, 3, [&](uint64_t L, const std::vector<int>& taken) {
         PairPass P;
         std::memset(&P, 0, sizeof(P));
@@ -435,7 +443,12 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan)
         PassPairs pp;
         for (int i : taken) {
             const EOp& e = ops[i];
-            if (e.form == F_CX) {
+            if (e.form == F_M4) {                       // both qubits local (pass cut)
+                const Mat4& src = (*mats)[e.mat];
+                M4 m;
+                for (int k = 0; k < 16; k++) m[k] = cplx(src[2 * k], src[2 * k + 1]);
+                pp.add_m4(pos_of[e.q], pos_of[e.c], m);
+            } else if (e.form == F_CX) {
                 const int t = pos_of[e.q], c = pos_of[e.c];
                 if (c >= 0) {
                     pp.add_cx(c, t);

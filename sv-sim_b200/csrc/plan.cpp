@@ -32,12 +32,18 @@ inline uint64_t bit(int q) { return 1ull << q; }
 struct OpInfo {
     uint64_t touch;
     int need;      // qubit that must be local (and in registers), or -1
+    int need2;     // a second qubit that must be local (F_M4), or -1
 };
 
 OpInfo info_of(const EOp& e, uint64_t all)
 {
     OpInfo r;
-    if (e.form == F_SRN) {
+    r.need2 = -1;
+    if (e.form == F_M4) {
+        r.touch = bit(e.q) | bit(e.c);
+        r.need = (int)e.q;
+        r.need2 = (int)e.c;
+    } else if (e.form == F_SRN) {
         // SRN_GATE (:894-907) as coded maps a to 0.5 (a0 + conj(a1), conj(a0) + a1):
         // it is only real-linear, so it does not commute with a complex gate on any
         // other qubit.  It is ordered against every op of the circuit.
@@ -233,11 +239,13 @@ void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
                 if (blocked == all) break;
                 continue;
             }
-            const int q = inf[i].need;
-            if (q >= 0 && !((L >> q) & 1)) {
-                if (nL < M) {
-                    L |= bit(q);
-                    nL++;
+            const int q = inf[i].need, q2 = inf[i].need2;
+            const int extra = (q >= 0 && !((L >> q) & 1)) + (q2 >= 0 && !((L >> q2) & 1));
+            if (extra > 0) {
+                if (nL + extra <= M) {
+                    if (q >= 0) L |= bit(q);
+                    if (q2 >= 0) L |= bit(q2);
+                    nL += extra;
                 } else {
                     blocked |= t;
                     if (blocked == all) break;

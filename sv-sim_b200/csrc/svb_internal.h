@@ -2,6 +2,7 @@
 // the device-side descriptors and the handle.
 #pragma once
 
+#include <array>
 #include <cstdint>
 #include <cstddef>
 #include <string>
@@ -39,6 +40,8 @@ enum Form : uint8_t {
     F_DIAG,     // diag(d0, d1), m = d0r d0i d1r d1i (adjoint inverses only)
     // two-qubit
     F_CX,       // CX_GATE :779      swap (c=1,t=0) <-> (c=1,t=1)
+    F_M4,       // general 4x4 complex matrix on (q: bit 0, c: bit 1), entries in a side
+                // table (EOp::mat); density-matrix superoperators; pair and per-gate only
     F_COUNT
 };
 
@@ -47,7 +50,8 @@ __host__ __device__ inline bool form_is_diag(int f) { return f >= F_Z && f <= F_
 struct EOp {
     uint8_t form = F_C1;
     uint32_t q = 0;        // target (dense, CX) or the qubit of a diagonal op
-    uint32_t c = 0;        // control (CX)
+    uint32_t c = 0;        // control (CX); second qubit (F_M4)
+    int32_t mat = -1;      // F_M4: index of its 4x4 matrix in the circuit's matrix table
     double m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     // --- adjoint bookkeeping ---
     int32_t gate = -1;     // index of the source gate
@@ -166,8 +170,12 @@ struct PairPlan {
     size_t n_blocks = 0, n_swaps = 0, n_relayouts = 0;
 };
 
-// Builds the pair plan; false if an op cannot be written as a matrix (SRN).
-bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan);
+// 4x4 complex matrix of an F_M4 op, row-major, re/im interleaved (index a = bit0 + 2 bit1)
+using Mat4 = std::array<double, 32>;
+
+// Builds the pair plan; false if an op cannot be written as a matrix (SRN).  `mats` holds
+// the matrices of F_M4 ops.
+bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::vector<Mat4>* mats = nullptr);
 
 struct DevPairBuffers {
     PairPass* passes = nullptr;
@@ -348,9 +356,21 @@ struct Sim {
     MeasureScratch mscr;
     double* d_small = nullptr;     // a few doubles for reduction results
     AdjScratch adj;
+    std::vector<Mat4> mats;        // matrices of F_M4 ops of the current circuit
+    uint32_t dm_qubits = 0;        // density-matrix handle: qubits of rho (state has 2x)
 };
 
 void set_error(const std::string& msg);
+
+// Plans and uploads an already lowered circuit on the handle (svb_set_circuit after its
+// validation and lowering; the density-matrix entry point with its superoperator blocks).
+svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* gates, size_t n_gates,
+                               double sweeps);
+// qubit slots a reference op uses (0 for an unknown op)
+int gate_qubit_slots(uint32_t op);
+// one general 4x4 block (F_M4) as a per-gate sweep
+template <typename T>
+cudaError_t launch_m4(void* state, int n, int q0, int q1, const Mat4& m, cudaStream_t s);
 
 }  // namespace svb
 

@@ -77,6 +77,9 @@ _SIGS = {
     "svb_apply_controlled": ([_vp, ctypes.c_uint32, ctypes.c_uint64, _dp, _vp], ctypes.c_int),
     "svb_measure_qubit": ([_vp, ctypes.c_uint32, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_int),
                            _dp], ctypes.c_int),
+    "svb_dm_create": ([ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+    "svb_dm_set_circuit": ([_vp, _vp, ctypes.c_size_t, _dp, ctypes.c_uint32], ctypes.c_int),
+    "svb_dm_probabilities": ([_vp, _dp], ctypes.c_int),
     "svb_last_error": ([], ctypes.c_char_p),
     "svb_version": ([], ctypes.c_char_p),
 }
