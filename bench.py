@@ -36,6 +36,7 @@ import numpy as np  # noqa: E402
 N_QUBITS = 30
 DEPTH = 40
 SEED = 2024
+FUSION_WIDTH = 4        # qubits per fused block of the tensor-core FP32 form
 METRIC = "n=30 gates/s & HBM GB/s: FP64 per-gate vs fused TC (1-F≤1e-6); adjoint grads/s"
 UNIT = "gates/s"
 WORKLOAD = "random circuit n=30 depth 40 (U3 all qubits + 15 CX random matching per layer), FP64"
@@ -59,6 +60,8 @@ def parse():
                     help="headline: the FP64 n=30 step (the measured line); the others run one "
                          "secondary form alone (for profiling and capacity runs)")
     ap.add_argument("--instances", type=int, default=512, help="QAOA batch size (--form qaoa)")
+    ap.add_argument("--fusion-width", type=int, default=FUSION_WIDTH, choices=[3, 4, 5],
+                    help="qubits per fused block of the tensor-core FP32 form")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="state precision of --form qaoa")
     return ap.parse_args()
@@ -326,10 +329,11 @@ def run_ours(args):
         print(json.dumps(out))
 
 
-def fused_form(device, circuit, k=5, reps=3, n=N_QUBITS):
+def fused_form(device, circuit, k=None, reps=3, n=N_QUBITS):
     """The same circuit on an FP32 state through the fused tensor-core engine, with its
     fidelity and largest amplitude error against the FP64 staged result."""
     import torch
+    k = FUSION_WIDTH if k is None else k
     from svsim_b200 import _native as nat
     h64 = nat.Handle(n, device, nat.SVB_FP64)
     h64.set_engine(nat.ENGINE_STAGED, 12 if n >= 20 else 0, 0)
@@ -361,7 +365,8 @@ def fused_form(device, circuit, k=5, reps=3, n=N_QUBITS):
            "hbm_frac_of_peak": info.moved_bytes / s / 1e9 / peak,
            "one_minus_fidelity_vs_fp64": 1.0 - fid, "max_abs_amp_err_vs_fp64": maxd,
            "norm_minus_one": norm32 - 1.0,
-           "kernel": "k_fused<5>: split-TF32 tcgen05.mma (M=128, N=K=64), TMEM accumulators"}
+           "kernel": f"k_fused<{k}>: split-TF32 tcgen05.mma (M=128, N=K={2 << k}), A operand and "
+                     "accumulators in TMEM, two tiles in flight"}
     del h32
     torch.cuda.empty_cache()
     return out
@@ -504,7 +509,7 @@ def run_form(args):
         circuit = None
         from svsim_b200 import circuits
         circuit = circuits.random_matching_circuit(args.qubits, DEPTH, seed=SEED)
-        res = fused_form(local, circuit, n=args.qubits, reps=max(1, args.steps))
+        res = fused_form(local, circuit, k=args.fusion_width, n=args.qubits, reps=max(1, args.steps))
     elif args.form == "qaoa":
         res = qaoa_form(local, args.instances, args.precision, reps=max(1, args.steps))
     else:

@@ -103,7 +103,6 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
     plan = FusedPlan{};
     plan.k = k;
     const int M = FT_TILE_BITS, G = FT_LOW_BITS;
-    const int rows = 1 << (M - k);
     const int N = 1 << (k + 1);
     const size_t N_ops = ops.size();
     const uint64_t all = (n >= 64) ? ~0ull : (bit(n) - 1);
@@ -189,71 +188,130 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
         }
         const int nblocks = (int)pblocks.size();
 
-        // Bit orderings.  The threads that write block f's operand have lane bits 0..3 on
-        // the local positions W_f (the tile loader's positions 1..4 for f = 0, otherwise
-        // row bits 0..3 of block f-1).  Their 8-byte stores are conflict-free when W_f lands
-        // on {target bit 0, row bits 0..2} of block f, so those come first.
+        // Bit orderings, chosen so that the kernel's 8-byte shared-memory accesses are
+        // conflict-free: the 16 lanes of a half warp (local positions = row bits 0..3 of
+        // the accessing block) must land on 16 distinct bank pairs (word bits 0..3).
+        //  * Block f > 0 is written from block f-1's rows: W = C[f-1][0..3] is matched onto
+        //    the four bank-pair images of fused_slot (image i from target slot tslot[i] or
+        //    row slot cslot[i]); a perfect matching always exists.
+        //  * Block 0 is gathered from the raw tile and the last block writes the output
+        //    stage; both layouts are chosen afterwards to fit (raw_xor, out_xor below).
+        //    Block 0 puts position 0 (the only source of word bit 0 in the raw tile) on a
+        //    row lane when it is a row.
         std::vector<std::vector<int>> T(nblocks), C(nblocks);
-        std::vector<int> W = {1, 2, 3, 4};
+        const int tslot[4] = {0, 1, 2, k >= 4 ? 3 : -1};
+        const int cslot[4] = {3, k >= 4 ? 0 : 1, k >= 4 ? 1 : 2, k >= 4 ? 2 : 0};
         for (int f = 0; f < nblocks; f++) {
             uint32_t tmask = 0;
             for (int q : pblocks[f].tq) tmask |= 1u << pos_of[q];
+            auto is_target = [&](int p) { return ((tmask >> p) & 1) != 0; };
             std::vector<int>& t = T[f];
             std::vector<int>& c = C[f];
-            for (int p : W)
-                if (((tmask >> p) & 1) && t.empty()) t.push_back(p);
-            for (int p = 0; p < M; p++)
-                if (((tmask >> p) & 1) && std::find(t.begin(), t.end(), p) == t.end()) t.push_back(p);
-            for (int p : W)
-                if (!((tmask >> p) & 1)) c.push_back(p);
-            for (int p = 0; p < M; p++)
-                if (!((tmask >> p) & 1) && std::find(c.begin(), c.end(), p) == c.end()) c.push_back(p);
-            W.assign(c.begin(), c.begin() + 4);
+            t.assign(k, -1);
+            c.assign(M - k, -1);
+            std::vector<char> used(M, 0);
+            if (f > 0) {
+                const int* W = C[f - 1].data();
+                int perm[4] = {0, 1, 2, 3}, best[4] = {0, 1, 2, 3}, best_ok = -1;
+                do {
+                    int good = 0;
+                    for (int j = 0; j < 4; j++) good += !is_target(W[j]) || tslot[perm[j]] >= 0;
+                    if (good > best_ok) {
+                        best_ok = good;
+                        std::copy(perm, perm + 4, best);
+                    }
+                } while (best_ok < 4 && std::next_permutation(perm, perm + 4));
+                for (int j = 0; j < 4; j++) {
+                    const int p = W[j], i = best[j];
+                    if (is_target(p) && tslot[i] >= 0) { t[tslot[i]] = p; used[p] = 1; }
+                    else if (!is_target(p)) { c[cslot[i]] = p; used[p] = 1; }
+                }
+            } else if (!is_target(0)) {
+                c[0] = 0;
+                used[0] = 1;
+            }
+            int ti = 0, ci = 0;
+            for (int p = 0; p < M; p++) {
+                if (used[p]) continue;
+                if (is_target(p)) {
+                    while (t[ti] >= 0) ti++;
+                    t[ti] = p;
+                } else {
+                    while (c[ci] >= 0) ci++;
+                    c[ci] = p;
+                }
+            }
         }
 
-        // per-block tables; offsets are additive over disjoint bit groups of the local index
-        auto operand_word = [&](int f, uint32_t l) -> uint32_t {
+        // Raw-tile and output-stage layouts: each local position p >= 4 (a run bit) gets a
+        // column of the run's XOR; positions 0..3 are fixed on word bits 0..3 (the raw
+        // tile cannot swizzle bit 0: a 16-byte copy keeps its two amplitudes in order).
+        // The columns of the accessing lanes' run-bit positions complete their fixed
+        // columns to independent ones.
+        auto choose_mix = [&](const std::vector<int>& lanes, uint32_t free_bits, uint8_t* col) {
+            uint32_t have = 0;
+            for (int j = 0; j < 4; j++)
+                if (lanes[j] < 4) have |= 1u << lanes[j];
+            for (int j = 0; j < 4; j++) {
+                if (lanes[j] < 4) continue;
+                for (int b = 0; b < 4; b++)
+                    if (((free_bits >> b) & 1) && !((have >> b) & 1)) {
+                        col[lanes[j] - 4] = (uint8_t)(1u << b);
+                        have |= 1u << b;
+                        break;
+                    }
+            }
+        };
+        uint8_t raw_col[8] = {0}, out_col[8] = {0};
+        choose_mix(C[0], 0xEu, raw_col);
+        choose_mix(C[nblocks - 1], 0xFu, out_col);
+        for (int r = 0; r < 256; r++) {
+            uint8_t rx = 0, ox = 0;
+            for (int b = 0; b < 8; b++)
+                if ((r >> b) & 1) { rx ^= raw_col[b]; ox ^= out_col[b]; }
+            P.raw_xor[r] = (uint8_t)(rx >> 1);      // on the chunk index (word bits 1..3)
+            P.out_xor[r] = ox;                      // on the word index (bits 0..3)
+        }
+        auto raw_word = [&](uint32_t l) { return l ^ ((uint32_t)P.raw_xor[l >> 4] << 1); };
+        auto out_word = [&](uint32_t l) { return l ^ (uint32_t)P.out_xor[l >> 4]; };
+
+        // per-block tables; the transpose slot is linear over GF(2) in the local index
+        auto slot_of = [&](int f, uint32_t l) -> uint32_t {
             uint32_t row = 0, a = 0;
             for (int i = 0; i < k; i++)
                 if ((l >> T[f][i]) & 1) a |= 1u << i;
             for (size_t i = 0; i < C[f].size(); i++)
                 if ((l >> C[f][i]) & 1) row |= 1u << i;
-            return kmajor_offset(row, 2 * a, rows) / 4;
+            return fused_slot(row, a, k);
         };
         std::vector<FusedBlock> fb(nblocks);
         for (int f = 0; f < nblocks; f++) {
             FusedBlock& B = fb[f];
             std::memset(&B, 0, sizeof(B));
+            const bool last = (f == nblocks - 1);
+            // local index bits of a target index / row bit group, and where they go next
+            auto place = [&](uint32_t l, uint16_t& raw, uint16_t& next) {
+                raw = (uint16_t)raw_word(l);
+                next = (uint16_t)(last ? out_word(l) : slot_of(f + 1, l));
+            };
             for (int a = 0; a < 64; a++) {
                 uint32_t l = 0;
                 for (int i = 0; i < k; i++)
                     if ((a >> i) & 1) l |= 1u << T[f][i];
-                B.a_sc[a] = (uint16_t)(a < (1 << k) ? l : 0);
+                if (a < (1 << k)) place(l, B.a_sc[a], B.nxt_a[a]);
             }
             for (int j = 0; j < 32; j++) {
                 uint32_t l = 0;
                 for (int i = 0; i < 5 && i < (int)C[f].size(); i++)
                     if ((j >> i) & 1) l |= 1u << C[f][i];
-                B.n_lo[j] = (uint16_t)l;
+                place(l, B.n_lo[j], B.nxt_nlo[j]);
             }
             for (int j = 0; j < 16; j++) {
                 uint32_t l = 0;
                 for (int i = 0; i < 4 && 5 + i < (int)C[f].size(); i++)
                     if ((j >> i) & 1) l |= 1u << C[f][5 + i];
-                B.n_hi[j] = (uint16_t)l;
+                place(l, B.n_hi[j], B.nxt_nhi[j]);
             }
-            for (int j = 0; j < 64; j++) {
-                B.off_lo[j] = operand_word(f, (uint32_t)j);
-                B.off_hi[j] = operand_word(f, (uint32_t)j << 6);
-            }
-        }
-        for (int f = 0; f < nblocks; f++) {
-            FusedBlock& B = fb[f];
-            const bool last = (f == nblocks - 1);
-            auto nxt = [&](uint32_t l) -> uint32_t { return last ? l : operand_word(f + 1, l); };
-            for (int a = 0; a < 64; a++) B.nxt_a[a] = nxt(B.a_sc[a]);
-            for (int j = 0; j < 32; j++) B.nxt_nlo[j] = nxt(B.n_lo[j]);
-            for (int j = 0; j < 16; j++) B.nxt_nhi[j] = nxt(B.n_hi[j]);
         }
 
         // block matrices: gate operand B[m'][kk] for the real form, hi and lo planes
@@ -270,12 +328,13 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
                 for (int i : pblocks[f].ops) apply_small(ops[i], tpos, col);
                 for (int r = 0; r < d; r++) U[(size_t)r * d + c] = col[r];
             }
+            // the gate operand: G_hi in rows 0..N-1 and G_lo in rows N..2N-1 of one
+            // K-major operand, so one MMA of width 2N forms X_hi G_hi and X_hi G_lo and
+            // one of width N (rows 0..N-1) adds X_lo G_hi
             FusedBlock& B = fb[f];
-            const size_t plane = (size_t)N * N;
             B.gate_word = (uint32_t)plan.gates.size();
-            plan.gates.resize(plan.gates.size() + 2 * plane);
-            float* hi = plan.gates.data() + B.gate_word;
-            float* lo = hi + plane;
+            plan.gates.resize(plan.gates.size() + 2 * (size_t)N * N);
+            float* gop = plan.gates.data() + B.gate_word;
             for (int mp = 0; mp < N; mp++) {
                 const int ar = mp >> 1, cr = mp & 1;
                 for (int kk = 0; kk < N; kk++) {
@@ -287,9 +346,8 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
                     // hi = val to TF32, lo = the remainder to TF32 (both rounded to
                     // nearest, so the pair carries ~21 bits of the FP64 entry, unbiased)
                     const float h = tf32_hi((float)val);
-                    const uint32_t w = kmajor_offset(mp, kk, N) / 4;
-                    hi[w] = h;
-                    lo[w] = tf32_hi((float)(val - (double)h));
+                    gop[kmajor_offset(mp, kk, 2 * N) / 4] = h;
+                    gop[kmajor_offset(N + mp, kk, 2 * N) / 4] = tf32_hi((float)(val - (double)h));
                 }
             }
             plan.blocks.push_back(B);
@@ -298,7 +356,6 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
         P.n_blocks = nblocks;
         plan.passes.push_back(P);
     }
-    (void)rows;
 }
 
 }  // namespace svb

@@ -1,24 +1,38 @@
-// Fused tensor-core engine: tcgen05 MMAs on an FP32 state tile in shared memory.
+// Fused tensor-core engine: tcgen05 MMAs on FP32 state tiles held in tensor memory.
 //
-// One persistent CTA per SM (8 warps, two per TMEM lane quadrant) walks the tiles of a
-// pass; the next tile is loaded into registers while the current one is in the tensor
-// core.
-// For a tile of 4096 amplitudes (12 local qubits) and a fused block on k target qubits,
-// the tile is viewed as X[n][kk]: rows n = the 2^(12-k) values of the other local
-// qubits, kk = 2a + re/im for the 2^k target values a.  The block's real-form gate
-// G[m'][kk] (2^(k+1) square) is applied as
+// A pass applies its fused blocks to every tile of 4096 amplitudes (12 local qubits).
+// For a block on k target qubits the tile is viewed as X[n][kk]: rows n = the 2^(12-k)
+// values of the other local qubits, kk = 2a + re/im for the 2^k target values a.  The
+// block's real-form gate G[m'][kk] (N = 2^(k+1) square) is applied as
 //        D[n][m'] = sum_kk X[n][kk] G[m'][kk]
-// with tcgen05.mma.kind::tf32 (M = 128 rows per MMA, N = 2^(k+1), K = 8 per
-// instruction) accumulating in TMEM, in three products X_hi G_hi + X_hi G_lo + X_lo G_hi
-// (split TF32: hi = x rounded to TF32, lo = x - hi rounded to TF32), so the result keeps ~FP32
-// accuracy.  Both operands sit in shared memory in the canonical K-major, no-swizzle
-// layout (8-row x 16-byte core matrices).  Each thread then reads its D row (one row n,
-// all 2^k amplitudes) with tcgen05.ld and scatters it, split again into hi/lo, into the
-// operand layout of the next block — or, after the last block, into a plain staging
-// copy of the tile that is written back to HBM.
+// with tcgen05.mma.kind::tf32 (M = 128 rows per MMA, K = 8 per instruction) in three
+// products X_hi G_hi + X_hi G_lo + X_lo G_hi (split TF32: hi = x rounded to TF32, lo =
+// the remainder rounded to TF32), so the result keeps ~FP32 accuracy.  The gate operand
+// holds G_hi in rows 0..N-1 and G_lo in rows N..2N-1, so per K step one MMA of width 2N
+// forms [X_hi G_hi | X_hi G_lo] and one of width N adds X_lo G_hi to the first half.
 //
-// Every wait on the MMA-completion mbarrier is bounded; on timeout the kernel records
-// an error, releases its tensor memory and returns.
+// One persistent CTA per SM: 8 warps (two per TMEM lane quadrant) move the data and one
+// warp issues the MMAs.
+//  * The state operand (hi and lo planes) lives in tensor memory as the MMA's A operand;
+//    only the gate operand (B, canonical K-major layout, no swizzle) is read from shared
+//    memory.  With both operands in shared memory the MMAs of a narrow block read more
+//    bytes per cycle than shared memory delivers.
+//  * After a block each thread reads its D rows (tcgen05.ld), adds the two halves, writes
+//    them into a transpose buffer in the next block's row order (fused_slot), reads back its rows of the next block, splits
+//    them into hi/lo and stores them into tensor memory (tcgen05.st).  Each warp then
+//    arrives on the slot's "operands ready" mbarrier, on which the MMA warp waits.
+//  * Two tiles are in flight, in two TMEM slots of 256 columns (A hi, A lo: 64 each; D:
+//    128): while the threads turn one tile's D into the next operand, the tensor core
+//    runs the other tile's MMAs.
+//  * Tiles arrive by 16-byte cp.async (the 4 lowest qubits are always local: 128-byte
+//    runs) into prefetch buffers some tiles ahead, each thread's copies completing on
+//    the buffer's mbarrier, and leave by 16-byte stores from the transpose buffer used
+//    as an output stage.  The layouts of both (per-run XOR swizzles the planner picks)
+//    and of the transpose buffer keep every 8- and 16-byte shared-memory access of the
+//    kernel free of bank conflicts wherever the pass's bit layout allows.
+// Every mbarrier wait is bounded and gives up early when another warp has given up; the
+// kernel then records an error, waits (bounded) for its MMAs and copies in flight,
+// releases its tensor memory and returns.
 #include <cstdint>
 
 #include "svb_internal.h"
@@ -26,7 +40,8 @@
 namespace svb {
 namespace {
 
-constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kTmemCols = 512;      // two slots
+constexpr uint32_t kSlotCols = 256;
 constexpr uint32_t kWaitLimit = 1u << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -49,18 +64,6 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes
 __host__ __device__ constexpr uint32_t umma_idesc_tf32(uint32_t n)
 {
     return (1u << 4) | (2u << 7) | (2u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
-                                         uint32_t accumulate)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-        :
-        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate),
-          "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t* bar)
@@ -117,88 +120,222 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-template <int K>
-struct FusedSmem {
-    static constexpr uint32_t x_bytes = 4096u * 2u * 4u;                  // one plane: 32 KiB
-    static constexpr uint32_t n_real = 1u << (K + 1);
-    static constexpr uint32_t gate_bytes = 2u * n_real * n_real * 4u;     // hi + lo planes
-    static constexpr uint32_t max_blocks = (uint32_t)fused_max_blocks(K);
-    static constexpr uint32_t x_hi = 0;
-    static constexpr uint32_t x_lo = x_hi + x_bytes;
-    static constexpr uint32_t gates = x_lo + x_bytes;
-    static constexpr uint32_t blocks = gates + max_blocks * gate_bytes;
-    static constexpr uint32_t pass = blocks + max_blocks * sizeof(FusedBlock);
-    static constexpr uint32_t misc = pass + sizeof(FusedPass);
-    static constexpr uint32_t total = misc + 64;
-    static constexpr int ctas_per_sm = total <= 113u * 1024u ? 2 : 1;
-    static_assert(gates % 16 == 0 && blocks % 16 == 0 && pass % 16 == 0 && misc % 16 == 0, "align");
-};
 
-// Writes amplitude (re, im) at word offset w of the state operand (re and im are adjacent
-// K values, 8-byte aligned), split into a TF32 hi plane and a TF32 lo plane.  Both
-// parts are rounded to nearest explicitly: the MMA reads only the upper 19 bits of each
-// FP32 word, and a remainder left in full FP32 would lose its low bits by truncation,
-// i.e. always towards zero, which shrinks the norm a little at every block.
-__device__ __forceinline__ void put_operand(float* xh, float* xl, uint32_t w, float re, float im)
+// D[tmem] (+)= A[tmem] . B[smem]
+__device__ __forceinline__ void mma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t idesc,
+                                            uint32_t accumulate)
 {
-    const float hr = tf32_rna(re), hi = tf32_rna(im);
-    *reinterpret_cast<float2*>(xh + w) = make_float2(hr, hi);
-    *reinterpret_cast<float2*>(xl + w) = make_float2(tf32_rna(re - hr), tf32_rna(im - hi));
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "r"(tmem_a), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const float* v)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"
+                 :: "r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])),
+                    "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])),
+                    "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v)
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+        :: "r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+           "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+           "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+           "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+           "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+           "r"(__float_as_uint(v[15]))
+        : "memory");
+}
+
+// W consecutive TMEM columns of this warp's 32 lanes (W = 8, 16 or 32)
+template <int W>
+__device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, float* v)
+{
+    if constexpr (W == 8) {
+        tmem_ld8(taddr, v);
+    } else {
+#pragma unroll
+        for (int c = 0; c < W; c += 16) tmem_ld16(taddr + (uint32_t)c, v + c);
+    }
+}
+
+template <int W>
+__device__ __forceinline__ void tmem_st_cols(uint32_t taddr, const float* v)
+{
+    if constexpr (W == 8) {
+        tmem_st8(taddr, v);
+    } else {
+#pragma unroll
+        for (int c = 0; c < W; c += 16) tmem_st16(taddr + (uint32_t)c, v + c);
+    }
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+
+// bounded wait that also gives up once *abort is set; a wait that runs out sets it
+__device__ __forceinline__ bool mbar_wait_abort(uint64_t* bar, uint32_t parity, volatile int* abort)
+{
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t it = 0; it < kWaitLimit; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+        if ((it & 31u) == 31u && *abort) return false;
+    }
+    *abort = 1;
+    return false;
+}
+
+// barrier of the 8 data warps (named barrier 1) that also ANDs a predicate over them
+__device__ __forceinline__ bool epi_sync_and(bool p)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred a, b;\n\t"
+        "setp.ne.u32 a, %1, 0;\n\t"
+        "bar.red.and.pred b, 1, %2, a;\n\t"
+        "selp.u32 %0, 1, 0, b;\n\t}\n"
+        : "=r"(r) : "r"(p ? 1u : 0u), "n"(FT_EPI_WARPS * 32) : "memory");
+    return r != 0;
+}
+
+// 16 bytes global -> shared, asynchronous (L2 only)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// arrive on the mbarrier once all of this thread's earlier cp.async copies have landed
+__device__ __forceinline__ void cp_async_arrive(uint64_t* bar)
+{
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" :: "r"(smem_u32(bar)) : "memory");
 }
 
 template <int K>
-__global__ void __launch_bounds__(FT_THREADS, FusedSmem<K>::ctas_per_sm)
+struct FusedSmem {
+    static constexpr uint32_t tile_bytes = 4096u * 8u;                    // 32 KiB
+    static constexpr uint32_t n_real = 1u << (K + 1);
+    static constexpr uint32_t gate_bytes = 2u * n_real * n_real * 4u;     // [G_hi; G_lo]
+    static constexpr uint32_t max_blocks = (uint32_t)fused_max_blocks(K);
+    static constexpr uint32_t n_raw = (uint32_t)fused_raw_buffers(K);
+    static constexpr uint32_t trans = 0;                                  // two transpose buffers
+    static constexpr uint32_t raw = trans + 2 * tile_bytes;               // prefetch buffers
+    static constexpr uint32_t gates = raw + n_raw * tile_bytes;
+    static constexpr uint32_t blocks = gates + max_blocks * gate_bytes;
+    static constexpr uint32_t pass = blocks + max_blocks * sizeof(FusedBlock);
+    static constexpr uint32_t tbase = pass + sizeof(FusedPass);          // tile index -> base, 3 x 256
+    static constexpr uint32_t misc = tbase + 3u * 256u * 8u;              // mbarriers, flags, counters
+    static constexpr uint32_t total = misc + 128;
+    static_assert(total <= 227u * 1024u, "shared memory of one CTA");
+    // a second CTA on the SM would wait for the 512 TMEM columns this one holds
+    static_assert(total > 114u * 1024u, "one CTA per SM");
+    static_assert(gates % 128 == 0 && blocks % 16 == 0 && pass % 16 == 0 && tbase % 16 == 0 &&
+                  misc % 16 == 0, "align");
+};
+
+template <int K>
+__global__ void __launch_bounds__(FT_THREADS, 1)
 k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
         const FusedBlock* __restrict__ blocks, const float* __restrict__ gates, int pass_index,
         uint64_t tiles, int* __restrict__ err)
 {
-    constexpr int N = 1 << (K + 1);                 // real gate dimension = MMA N = K extent
+    constexpr int N = 1 << (K + 1);                 // real gate dimension = K extent
+    constexpr int DN = 2 * N;                       // D columns per M block: [hi | lo products]
     constexpr int ROWS = 1 << (FT_TILE_BITS - K);   // rows of the state operand
     constexpr int MBLK = ROWS / 128;                // M = 128 blocks
     constexpr int KSTEPS = N / 8;                   // tf32 MMA K = 8
-    constexpr int HALF = N / 2;                     // TMEM columns read per thread and M block
-    constexpr uint32_t GATE_WORDS = 2u * N * N;     // hi + lo planes
-    constexpr uint32_t IDESC = umma_idesc_tf32(N);
-    constexpr int PAIRS = 4096 / 2 / FT_THREADS;    // float4 (2 amplitudes) per thread
-    static_assert(MBLK * N <= (int)kTmemCols, "TMEM columns");
+    constexpr int HALF = N / 2;                     // columns per thread and M block
+    constexpr int HAMP = HALF / 2;                  // amplitudes per thread and M block
+    constexpr int CPR = (1 << K) / 2;               // 16-byte chunks per transpose row
+    constexpr int EPI = FT_EPI_WARPS * 32;          // data threads
+    constexpr uint32_t GATE_WORDS = 2u * N * N;
+    constexpr uint32_t IDESC_W = umma_idesc_tf32(DN), IDESC_N = umma_idesc_tf32(N);
+    constexpr uint32_t PLANE = (uint32_t)(MBLK * N);   // TMEM columns of one operand plane
+    using L = FusedSmem<K>;
+    constexpr uint32_t NR = L::n_raw;
+    static_assert(2 * PLANE + MBLK * DN <= kSlotCols && 2 * kSlotCols <= kTmemCols, "TMEM slots");
+    static_assert(HAMP % 2 == 0 && MBLK * HALF == 32 && EPI == 256, "thread share of a tile");
 
     extern __shared__ __align__(128) unsigned char sm[];
-    using L = FusedSmem<K>;
-    float* xh = reinterpret_cast<float*>(sm + L::x_hi);
-    float* xl = reinterpret_cast<float*>(sm + L::x_lo);
+    float2* trans = reinterpret_cast<float2*>(sm + L::trans);
+    float2* raw = reinterpret_cast<float2*>(sm + L::raw);
     float* sg = reinterpret_cast<float*>(sm + L::gates);
     FusedBlock* sb = reinterpret_cast<FusedBlock*>(sm + L::blocks);
     FusedPass* sp = reinterpret_cast<FusedPass*>(sm + L::pass);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::misc);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::misc + 16);
+    uint64_t* tb = reinterpret_cast<uint64_t*>(sm + L::tbase);
+    uint64_t* bar_mma = reinterpret_cast<uint64_t*>(sm + L::misc);   // per slot: MMAs done
+    uint64_t* bar_ready = bar_mma + 2;                               // per slot: operands stored
+    uint64_t* bar_load = bar_ready + 2;                              // per prefetch buffer
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::misc + 64);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::misc + 68);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(sm + L::misc + 72);  // [0,2) MMAs committed,
+    // [2,4) MMAs consumed, [4,4+NR) loads issued, [6,6+NR) loads consumed
 
     const int tid = threadIdx.x;
-    const int warp = tid >> 5;
-    const int quad = warp & 3;          // TMEM lane quadrant of this warp
-    const int half = warp >> 2;         // which half of the D columns it reads
+    const int warp = tid >> 5, lane = tid & 31;
+    const bool mma_warp = warp == FT_EPI_WARPS;
+    const int quad = warp & 3;          // TMEM lane quadrant of a data warp
+    const int half = (warp >> 2) & 1;   // which half of the columns it handles
+    const uint64_t my_tiles = blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     // -- stage the pass, its blocks and their gate operands in shared memory
     {
-        const FusedPass& gp = passes[pass_index];
-        const uint4* src = reinterpret_cast<const uint4*>(&gp);
+        const uint4* src = reinterpret_cast<const uint4*>(passes + pass_index);
         uint4* dst = reinterpret_cast<uint4*>(sp);
         for (int w = tid; w < (int)(sizeof(FusedPass) / 16); w += FT_THREADS) dst[w] = src[w];
     }
     __syncthreads();
     const int nb = sp->n_blocks;
-    {
+    const bool plan_ok = nb >= 1 && nb <= (int)L::max_blocks && sp->n_nonlocal <= FT_MAX_NONLOCAL;
+    if (plan_ok) {
         const uint4* src = reinterpret_cast<const uint4*>(blocks + sp->block_begin);
         uint4* dst = reinterpret_cast<uint4*>(sb);
         for (int w = tid; w < nb * (int)(sizeof(FusedBlock) / 16); w += FT_THREADS) dst[w] = src[w];
+        // tile index bits 8t..8t+7 -> their share of the tile's global base
+        for (int i = tid; i < 3 * 256; i += FT_THREADS) {
+            const int t = i >> 8;
+            uint64_t base = 0;
+            for (int b = 0; b < 8; b++) {
+                const int q = 8 * t + b;
+                if (q < sp->n_nonlocal && ((i >> b) & 1)) base |= 1ull << sp->nonlocal_q[q];
+            }
+            tb[i] = base;
+        }
     }
     __syncthreads();
-    for (int b = 0; b < nb; b++) {
+    for (int b = 0; plan_ok && b < nb; b++) {
         const uint4* src = reinterpret_cast<const uint4*>(gates + sb[b].gate_word);
         uint4* dst = reinterpret_cast<uint4*>(sg + b * GATE_WORDS);
         for (int w = tid; w < (int)(GATE_WORDS / 4); w += FT_THREADS) dst[w] = src[w];
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(bar)) : "memory");
+        mbar_init(bar_mma, 1);
+        mbar_init(bar_mma + 1, 1);
+        mbar_init(bar_ready, FT_EPI_WARPS);
+        mbar_init(bar_ready + 1, FT_EPI_WARPS);
+        for (uint32_t i = 0; i < NR; i++) mbar_init(bar_load + i, EPI);
+        *abort_flag = 0;
+        for (int i = 0; i < 8; i++) counts[i] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -211,127 +348,244 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
-    const uint32_t x_hi_a = smem_u32(xh), x_lo_a = smem_u32(xl), g_a = smem_u32(sg);
     const FusedPass& P = *sp;
-    uint32_t parity = 0;
-    bool ok = true;
+    const bool run = plan_ok && my_tiles > 0;
 
-    auto tile_base = [&](uint64_t tile) {
-        uint64_t base = 0;
-        for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
-        return base;
+    // global amplitude offset of this CTA's j-th tile
+    auto tile_base = [&](uint64_t j) {
+        const uint64_t t = blockIdx.x + j * gridDim.x;
+        return tb[t & 255u] | tb[256 + ((t >> 8) & 255u)] | tb[512 + ((t >> 16) & 255u)];
     };
-    // thread t owns the amplitude pairs at local indices 2 (t + 256 j), j < PAIRS; the
-    // lowest local qubit is global qubit 0, so each pair is 16 contiguous bytes.  Their
-    // global offsets and their places in block 0's operand are fixed for the pass.
-    uint64_t gof[PAIRS];
-    uint32_t w0[PAIRS][2];
-#pragma unroll
-    for (int j = 0; j < PAIRS; j++) {
-        const uint32_t l = 2u * ((uint32_t)tid + (uint32_t)FT_THREADS * (uint32_t)j);
-        gof[j] = P.g_lo[l & 63u] + P.g_hi[l >> 6];
-        w0[j][0] = sb[0].off_lo[l & 63u] + sb[0].off_hi[l >> 6];
-        w0[j][1] = sb[0].off_lo[(l + 1) & 63u] + sb[0].off_hi[(l + 1) >> 6];
-    }
-    float4 cur[PAIRS];
-    uint64_t base = tile_base(blockIdx.x);
-    if (blockIdx.x < tiles) {
-#pragma unroll
-        for (int j = 0; j < PAIRS; j++) cur[j] = *reinterpret_cast<const float4*>(sv + base + gof[j]);
-    }
 
-    for (uint64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        // block 0 operand from the registers
-#pragma unroll
-        for (int j = 0; j < PAIRS; j++) {
-            put_operand(xh, xl, w0[j][0], cur[j].x, cur[j].y);
-            put_operand(xh, xl, w0[j][1], cur[j].z, cur[j].w);
-        }
-        // prefetch the next tile while this one is in the tensor core
-        const uint64_t next = tile + gridDim.x;
-        const uint64_t nbase = next < tiles ? tile_base(next) : 0;
-        if (next < tiles) {
-#pragma unroll
-            for (int j = 0; j < PAIRS; j++) cur[j] = *reinterpret_cast<const float4*>(sv + nbase + gof[j]);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-
-        for (int b = 0; b < nb && ok; b++) {
-            if (tid == 0) {
+    if (mma_warp) {
+        // ---- the MMA warp: one lane issues each slot's blocks once its operands are stored
+        if (lane == 0 && run) {
+            const uint32_t g_a = smem_u32(sg);
+            auto issue = [&](int s, int b) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t gh = g_a + (uint32_t)b * GATE_WORDS * 4u;
-                const uint32_t gl = gh + (uint32_t)N * N * 4u;
+                const uint32_t base = tmem + (uint32_t)s * kSlotCols;
+                const uint32_t g = g_a + (uint32_t)b * GATE_WORDS * 4u;
 #pragma unroll
                 for (int mb = 0; mb < MBLK; mb++) {
-                    const uint32_t d = tmem + (uint32_t)(mb * N);
-                    const uint32_t aoff = (uint32_t)mb * 16u * 128u;
+                    const uint32_t d = base + 2u * PLANE + (uint32_t)(mb * DN);
+                    const uint32_t ah = base + (uint32_t)(mb * N), al = ah + PLANE;
 #pragma unroll
-                    for (int s = 0; s < KSTEPS; s++) {
-                        const uint32_t ka = (uint32_t)s * 2u * (ROWS * 16u);
-                        const uint32_t kb = (uint32_t)s * 2u * (N * 16u);
-                        const uint64_t dah = umma_desc(x_hi_a + aoff + ka, ROWS * 16u, 128u);
-                        const uint64_t dal = umma_desc(x_lo_a + aoff + ka, ROWS * 16u, 128u);
-                        const uint64_t dbh = umma_desc(gh + kb, N * 16u, 128u);
-                        const uint64_t dbl = umma_desc(gl + kb, N * 16u, 128u);
-                        mma_tf32(d, dah, dbh, IDESC, s > 0 ? 1u : 0u);
-                        mma_tf32(d, dah, dbl, IDESC, 1u);
-                        mma_tf32(d, dal, dbh, IDESC, 1u);
+                    for (int k8 = 0; k8 < KSTEPS; k8++) {
+                        // two 16-byte K chunks of the 2N-row operand per K step
+                        const uint64_t dg = umma_desc(g + (uint32_t)k8 * 2u * (DN * 16u), DN * 16u, 128u);
+                        mma_tf32_ts(d, ah + 8u * k8, dg, IDESC_W, k8 > 0 ? 1u : 0u);
+                        mma_tf32_ts(d, al + 8u * k8, dg, IDESC_N, 1u);
                     }
                 }
-                mma_commit(bar);
+                mma_commit(bar_mma + s);
+                counts[s]++;
+            };
+            uint32_t rpar0 = 0, rpar1 = 0;
+            int blk0 = 0, blk1 = 0;
+            bool act0 = true, act1 = my_tiles > 1;
+            uint64_t next = act1 ? 2 : 1;
+            bool live = mbar_wait_abort(bar_ready, 0, abort_flag);
+            if (live) { rpar0 = 1; issue(0, 0); }
+            if (live && act1) {
+                live = mbar_wait_abort(bar_ready + 1, 0, abort_flag);
+                if (live) { rpar1 = 1; issue(1, 0); }
             }
-            const bool got = mbar_wait(bar, parity);
-            parity ^= 1u;
-            ok = __syncthreads_and(got ? 1 : 0) != 0;
-            if (!ok) break;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // this warp's D rows n = 32 quad + lane + 128 mb, columns of its half
-            const FusedBlock& B = sb[b];
-            const bool last = (b == nb - 1);
-            float dv[MBLK][HALF];
+            // the data warps' order: slots alternate; a slot's next block, or block 0 of
+            // its next tile
+            auto step = [&](int s, bool& act, int& blk, uint32_t& rpar) {
+                if (!act || !live) return;
+                if (blk + 1 < nb) {
+                    blk++;
+                } else if (next < my_tiles) {
+                    next++;
+                    blk = 0;
+                } else {
+                    act = false;
+                    return;
+                }
+                live = mbar_wait_abort(bar_ready + s, rpar, abort_flag);
+                if (!live) return;
+                rpar ^= 1u;
+                issue(s, blk);
+            };
+            while (live && (act0 || act1)) {
+                step(0, act0, blk0, rpar0);
+                step(1, act1, blk1, rpar1);
+            }
+        }
+    } else if (run) {
+        // ---- the data warps
+        const uint32_t lane_base = (uint32_t)(quad * 32) << 16;
+        // the 8 16-byte chunks of a thread in a tile: chunk c = tid + 256 i is part tid & 7
+        // of run (tid >> 3) + 32 i (local index 16 run + 2 part)
+        const uint64_t g_part = P.g_lo[((tid >> 3) & 3) << 4] + 2u * (uint32_t)(tid & 7);
+        auto chunk_off = [&](int i) { return g_part + P.g_hi[(tid >> 5) + 8 * i]; };
+
+        // tile j into prefetch buffer j % NR (8 cp.async per thread, arriving on its mbarrier)
+        auto issue_load = [&](uint64_t j) {
+            const uint32_t rb = (uint32_t)(j % NR);
+            const float2* src = sv + tile_base(j);
+            float2* dst = raw + rb * 4096u;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const uint32_t c = (uint32_t)(tid + EPI * i);
+                cp_async16(dst + 2 * (c ^ P.raw_xor[c >> 3]), src + chunk_off(i));
+            }
+            cp_async_arrive(bar_load + rb);
+            if (tid == 0) counts[4 + rb]++;
+        };
+        // rows n = 128 mb + 32 quad + lane, columns half * HALF + [0, HALF): hi/lo into
+        // the A planes of slot s, then this warp's arrival on the slot's ready barrier
+        auto put_rows = [&](int s, float (&v)[MBLK][HALF]) {
+            const uint32_t base = tmem + (uint32_t)s * kSlotCols + lane_base + (uint32_t)(half * HALF);
 #pragma unroll
             for (int mb = 0; mb < MBLK; mb++) {
-                const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(mb * N + half * HALF);
-                if constexpr (HALF >= 16) {
+                float h[HALF], l[HALF];
 #pragma unroll
-                    for (int c = 0; c < HALF; c += 16) tmem_ld16(ta + (uint32_t)c, &dv[mb][c]);
-                } else {
-                    tmem_ld8(ta, &dv[mb][0]);
+                for (int i = 0; i < HALF; i++) {
+                    h[i] = tf32_rna(v[mb][i]);
+                    l[i] = tf32_rna(v[mb][i] - h[i]);
                 }
+                tmem_st_cols<HALF>(base + (uint32_t)(mb * N), h);
+                tmem_st_cols<HALF>(base + PLANE + (uint32_t)(mb * N), l);
+            }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_ready + s);
+        };
+
+        bool ok = true;
+        uint32_t mpar0 = 0, mpar1 = 0, tsel = 0;
+        int blk0 = 0, blk1 = 0;
+        uint64_t tj0 = 0, tj1 = 0, next_j = 0;
+        bool act0 = false, act1 = false;
+
+        // a new tile in slot s: its block-0 rows gathered from the prefetch buffer
+        auto start = [&](int s, uint64_t j) -> bool {
+            const uint32_t rb = (uint32_t)(j % NR);
+            const bool got = mbar_wait_abort(bar_load + rb, (uint32_t)((j / NR) & 1u), abort_flag);
+            const float2* R = raw + rb * 4096u;
+            const FusedBlock& B0 = sb[0];
+            float v[MBLK][HALF];
+#pragma unroll
+            for (int mb = 0; mb < MBLK; mb++) {
+                const uint32_t n = (uint32_t)(128 * mb + 32 * quad + lane);
+                const uint32_t rl = (uint32_t)B0.n_lo[n & 31u] ^ (uint32_t)B0.n_hi[n >> 5];
+#pragma unroll
+                for (int a2 = 0; a2 < HAMP; a2++) {
+                    const float2 x = R[rl ^ (uint32_t)B0.a_sc[half * HAMP + a2]];
+                    v[mb][2 * a2] = x.x;
+                    v[mb][2 * a2 + 1] = x.y;
+                }
+            }
+            // every thread's reads of the buffer are done before it is refilled
+            if (!epi_sync_and(got)) return false;
+            if (tid == 0) counts[6 + rb]++;
+            if (j + NR < my_tiles) issue_load(j + NR);
+            put_rows(s, v);
+            return true;
+        };
+
+        // one step of slot s: wait for its MMAs, then its next operand or its output
+        auto step = [&](int s, bool& act, int& blk, uint64_t& tj, uint32_t& mpar) {
+            if (!act || !ok) return;
+            const bool got = mbar_wait_abort(bar_mma + s, mpar, abort_flag);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            float v[MBLK][HALF], w[MBLK][HALF];
+            const uint32_t dcol = tmem + (uint32_t)s * kSlotCols + lane_base + 2u * PLANE + (uint32_t)(half * HALF);
+#pragma unroll
+            for (int mb = 0; mb < MBLK; mb++) {
+                tmem_ld_cols<HALF>(dcol + (uint32_t)(mb * DN), v[mb]);
+                tmem_ld_cols<HALF>(dcol + (uint32_t)(mb * DN + N), w[mb]);
             }
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncthreads();   // every row is read before the operand planes are overwritten
-            float2* stage = reinterpret_cast<float2*>(xh);     // plain tile copy after the last block
+#pragma unroll
+            for (int mb = 0; mb < MBLK; mb++)
+#pragma unroll
+                for (int i = 0; i < HALF; i++) v[mb][i] += w[mb][i];
+            const FusedBlock& B = sb[blk];
+            float2* T = trans + tsel * 4096u;
+            tsel ^= 1u;
+            // D rows into the transpose buffer: the next block's row order, or (last block)
+            // local-index order as the output stage
 #pragma unroll
             for (int mb = 0; mb < MBLK; mb++) {
-                const uint32_t n = (uint32_t)(quad * 32 + (tid & 31) + 128 * mb);
-                const uint32_t wn = B.nxt_nlo[n & 31u] + B.nxt_nhi[n >> 5];
+                const uint32_t n = (uint32_t)(128 * mb + 32 * quad + lane);
+                const uint32_t wn = (uint32_t)B.nxt_nlo[n & 31u] ^ (uint32_t)B.nxt_nhi[n >> 5];
 #pragma unroll
-                for (int a2 = 0; a2 < HALF / 2; a2++) {
-                    const int a = half * (HALF / 2) + a2;
-                    const uint32_t w = wn + B.nxt_a[a];
-                    const float re = dv[mb][2 * a2], im = dv[mb][2 * a2 + 1];
-                    if (last) stage[w] = make_float2(re, im);
-                    else put_operand(xh, xl, w, re, im);
+                for (int a2 = 0; a2 < HAMP; a2++)
+                    T[wn ^ (uint32_t)B.nxt_a[half * HAMP + a2]] = make_float2(v[mb][2 * a2], v[mb][2 * a2 + 1]);
+            }
+            if (!epi_sync_and(got)) { ok = false; return; }
+            mpar ^= 1u;
+            if (tid == 0) counts[2 + s]++;
+            const float4* t4 = reinterpret_cast<const float4*>(T);
+            if (blk + 1 < nb) {
+                // this thread's rows of the next block
+#pragma unroll
+                for (int mb = 0; mb < MBLK; mb++) {
+                    const uint32_t n = (uint32_t)(128 * mb + 32 * quad + lane);
+                    const bool swap = (n >> 3) & 1u;       // fused_slot swaps a chunk's amplitudes
+#pragma unroll
+                    for (int c2 = 0; c2 < HAMP / 2; c2++) {
+                        const uint32_t c = (uint32_t)(half * (HAMP / 2) + c2);
+                        const float4 x = t4[n * CPR + (c ^ fused_chunk_swizzle(n, K))];
+                        v[mb][4 * c2] = swap ? x.z : x.x;
+                        v[mb][4 * c2 + 1] = swap ? x.w : x.y;
+                        v[mb][4 * c2 + 2] = swap ? x.x : x.z;
+                        v[mb][4 * c2 + 3] = swap ? x.y : x.w;
+                    }
+                }
+                blk++;
+                put_rows(s, v);
+            } else {
+                // the tile out in 16-byte pieces (8 threads per 128-byte run)
+                float2* dst = sv + tile_base(tj);
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const uint32_t c = (uint32_t)(tid + EPI * i);
+                    const uint32_t ox = P.out_xor[c >> 3];
+                    float4 x = t4[c ^ (ox >> 1)];
+                    if (ox & 1u) x = make_float4(x.z, x.w, x.x, x.y);
+                    *reinterpret_cast<float4*>(dst + chunk_off(i)) = x;
+                }
+                if (next_j < my_tiles) {
+                    tj = next_j++;
+                    blk = 0;
+                    ok = start(s, tj);
+                } else {
+                    act = false;
                 }
             }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
+        };
+
+        for (uint64_t j = 0; j < NR && j < my_tiles; j++) issue_load(j);
+        tj0 = next_j++;
+        act0 = true;
+        ok = start(0, tj0);
+        if (ok && next_j < my_tiles) {
+            tj1 = next_j++;
+            act1 = true;
+            ok = start(1, tj1);
         }
-        if (!ok) break;
-        // store the tile
-        const float4* stage4 = reinterpret_cast<const float4*>(xh);
-#pragma unroll
-        for (int j = 0; j < PAIRS; j++)
-            *reinterpret_cast<float4*>(sv + base + gof[j]) = stage4[tid + FT_THREADS * j];
-        base = nbase;
-        __syncthreads();
+        while (ok && (act0 || act1)) {
+            step(0, act0, blk0, tj0, mpar0);
+            step(1, act1, blk1, tj1, mpar1);
+        }
+        if (!ok) *abort_flag = 1;
     }
-    if (!ok) {
-        if (tid == 0) atomicExch(err, 1);
-        mbar_wait(bar, parity ^ 1u);     // bounded: let an MMA still in flight finish
+
+    __syncthreads();
+    if (!plan_ok && tid == 0) atomicExch(err, 1);
+    if (*abort_flag && tid == 0) {
+        atomicExch(err, 1);
+        // let what is still in flight land before the memory goes away (bounded waits)
+        for (int s = 0; s < 2; s++)
+            for (uint32_t c = counts[2 + s]; c < counts[s]; c++) mbar_wait(bar_mma + s, c & 1u);
+        for (uint32_t rb = 0; rb < NR; rb++)
+            for (uint32_t c = counts[6 + rb]; c < counts[4 + rb]; c++) mbar_wait(bar_load + rb, c & 1u);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -351,13 +605,10 @@ cudaError_t launch_k(void* state, int n, int pass_index, const DevFusedBuffers& 
         cudaError_t e = cudaFuncSetAttribute(k_fused<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)FusedSmem<K>::total);
         if (e != cudaSuccess) return e;
-        int sms = 0, per_sm = 0;
+        int sms = 0;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<K>, FT_THREADS,
-                                                          FusedSmem<K>::total);
-        if (e != cudaSuccess) return e;
-        ctas[dev] = sms * (per_sm > 0 ? per_sm : 1);
+        ctas[dev] = sms;                 // one CTA per SM (all of its tensor memory)
     }
     const uint64_t tiles = 1ull << (n - FT_TILE_BITS);
     const uint64_t grid = tiles < (uint64_t)ctas[dev] ? tiles : (uint64_t)ctas[dev];

@@ -199,24 +199,57 @@ void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
 constexpr int FT_TILE_BITS = 12;     // 4096 FP32 amplitudes per tile (32 KiB)
 constexpr int FT_LOW_BITS = 4;       // the 4 lowest qubits are always local (128-byte runs)
 constexpr int FT_MAX_BLOCKS = 8;     // upper bound of fused blocks per pass
-// blocks per pass that fit in shared memory: k = 5 keeps one CTA per SM (4 gate
-// operands of 32 KiB); k <= 4 leaves room for two CTAs per SM
-__host__ __device__ constexpr int fused_max_blocks(int k) { return k >= 5 ? 4 : (k == 4 ? 5 : 8); }
-constexpr int FT_THREADS = 256;      // two warps per TMEM lane quadrant
+// Shared memory of a fused CTA: a transpose buffer, an output stage and the raw-tile
+// prefetch buffers (32 KiB each), then the pass's gate operands (hi + lo planes,
+// 2 (2^(k+1))^2 floats per block).  k = 5 keeps one prefetch buffer and 3 blocks; k <= 4
+// two buffers and 5 (k = 4) or 8 (k = 3) blocks, all inside the 227 KiB of one CTA.
+__host__ __device__ constexpr int fused_max_blocks(int k) { return k >= 5 ? 3 : (k == 4 ? 5 : 8); }
+__host__ __device__ constexpr int fused_raw_buffers(int k) { return k >= 5 ? 1 : 2; }
+constexpr int FT_EPI_WARPS = 8;      // warps that move tiles and operands: two per TMEM lane quadrant
+constexpr int FT_THREADS = 32 * (FT_EPI_WARPS + 1);   // plus one warp that issues the MMAs
+constexpr int FT_MAX_NONLOCAL = 24;  // tile-index bits of a pass (n <= 36)
 constexpr int FT_MIN_K = 3, FT_MAX_K = 5;
 
-struct FusedBlock {                  // 1200 bytes
-    uint16_t a_sc[64];               // target index a -> local index bits
-    uint16_t n_lo[32];               // row bits 0-4 -> local index bits
-    uint16_t n_hi[16];               // row bits 5-8 -> local index bits
-    uint32_t off_lo[64];             // local index bits 0-5 -> word offset in the state operand
-    uint32_t off_hi[64];             // local index bits 6-11 -> word offset
-    // where the amplitudes of this block's output rows go next: the word offset in the
-    // next block's operand, or (last block) the amplitude index in the plain tile copy;
-    // additive over the disjoint bit groups of the local index
-    uint32_t nxt_a[64];              // target index a
-    uint32_t nxt_nlo[32];            // row bits 0-4
-    uint32_t nxt_nhi[16];            // row bits 5-8
+// Shared-memory layouts of the fused kernel.  All are linear over GF(2) in the bits they
+// index, so tables of them combine by XOR.
+//
+// Raw tile (a prefetched tile) and output stage (a finished tile): the amplitude of local
+// index l sits at word (8-byte slot) l ^ raw_xor[l >> 4] << 1, resp. l ^ out_xor[l >> 4]:
+// per 128-byte run (16 amplitudes, local index bits 0..3 = qubits 0..3) an XOR on the
+// run's chunk index, resp. on its word index (which may swap the two amplitudes of a
+// 16-byte chunk).  The planner picks both per pass (FusedPass) so that the 16 threads of
+// a half warp that gather block 0's rows from the raw tile, or scatter the last block's
+// rows into the output stage, hit 16 distinct bank pairs.
+//
+// Transpose buffer: amplitude (row n, target index a) of a k-qubit block at word
+// fused_slot(n, a, k): rows of 2^k amplitudes; the 16-byte chunks of a row XOR-swizzled by
+// row bits so that the 8 threads of a quarter warp reading one chunk of 8 consecutive rows
+// hit 8 bank groups, and the two amplitudes of a chunk swapped by row bit 3.  The bank
+// pair of a word (its bits 0..3) takes image 0 from target bit 0 or row bit 3, and images
+// 1..3 from target bits 1..3 or row bits 0..2 (k >= 4); for k = 3 from target bits 1, 2 or
+// row bits 1, 2, and image 3 from row bit 0.
+__host__ __device__ constexpr uint32_t fused_chunk_swizzle(uint32_t n, int k)
+{
+    return k >= 4 ? (n & 7u) : ((n >> 1) & 3u);
+}
+__host__ __device__ constexpr uint32_t fused_slot(uint32_t n, uint32_t a, int k)
+{
+    return (n << k) | ((((a >> 1) ^ fused_chunk_swizzle(n, k)) << 1)) | ((a ^ (n >> 3)) & 1u);
+}
+
+struct FusedBlock {                  // 464 bytes
+    // where this block's input amplitudes sit in the raw tile (their word there; used for
+    // a pass's first block), XOR-combined over the target index and row bits 0-4 and 5-8
+    uint16_t a_sc[64];               // target index a
+    uint16_t n_lo[32];               // row bits 0-4
+    uint16_t n_hi[16];               // row bits 5-8
+    // where the amplitudes of this block's output rows go: their slot in the next
+    // block's transpose layout (fused_slot of the next block's (row, target index)), or,
+    // after the last block, their word in the output stage; XOR-combined over the target
+    // index and row bits 0-4 and 5-8
+    uint16_t nxt_a[64];              // target index a
+    uint16_t nxt_nlo[32];            // row bits 0-4
+    uint16_t nxt_nhi[16];            // row bits 5-8
     uint32_t gate_word;              // word offset of the gate operand (hi plane, then lo)
     uint32_t pad[3];
 };
@@ -227,6 +260,8 @@ struct FusedPass {
     uint8_t nonlocal_q[64 - FT_TILE_BITS];
     uint64_t g_lo[64];               // local index bits 0-5 -> global amplitude offset
     uint64_t g_hi[64];               // local index bits 6-11 -> global amplitude offset
+    uint8_t raw_xor[256];            // per run (local index >> 4): XOR on its chunk index in a raw tile
+    uint8_t out_xor[256];            // per run: XOR on its word index in the output stage
     int32_t n_nonlocal, block_begin, n_blocks, pad;
 };
 static_assert(sizeof(FusedPass) % 16 == 0, "FusedPass layout");

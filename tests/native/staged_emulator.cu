@@ -176,10 +176,14 @@ extern "C" int emu_plan_dump(uint32_t n, const svb_gate* gates, size_t n_gates, 
 }
 
 // ---- fused tensor-core plans ---------------------------------------------------------
-// Executes a fused plan on the CPU with the kernel's data flow: operand offsets from the
-// block tables, D[n][m'] = sum_kk X[n][kk] (G_hi + G_lo)[m'][kk] read through the
-// canonical K-major layout, rows scattered back through the a/n tables.  The MMA is
-// evaluated in FP64 here; only the layout and table logic are under test.
+// Executes a fused plan on the CPU with the kernel's data flow: block 0's rows gathered
+// from the raw tile (raw_xor layout) through the a/n tables; D[n][m'] =
+// sum_kk X[n][kk] (G_hi + G_lo)[m'][kk] with G_hi and G_lo read from rows m' and N + m'
+// of the 2N-row canonical K-major gate operand; each D row scattered through the
+// XOR-combined next tables into the transpose buffer (every slot written once) and the
+// next block's rows read back from it at fused_slot(n, a); the last block's rows
+// scattered into the output stage (out_xor layout).  The MMA is evaluated in FP64
+// here; only the layout and table logic are under test.
 static uint32_t emu_kmajor(uint32_t row, uint32_t kk, uint32_t rows)
 {
     return ((kk >> 2) * (rows * 16u) + (row >> 3) * 128u + (row & 7u) * 16u + (kk & 3u) * 4u) / 4u;
@@ -197,60 +201,75 @@ extern "C" int emu_fused_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
     plan_fused(eops, (int)n, k, plan);
     if (n_passes) *n_passes = plan.passes.size();
     if (n_blocks) *n_blocks = plan.blocks.size();
-    const int N = 1 << (k + 1), ROWS = 1 << (FT_TILE_BITS - k);
+    const int N = 1 << (k + 1), ROWS = 1 << (FT_TILE_BITS - k), A = 1 << k;
     const uint64_t tiles = 1ull << (n - FT_TILE_BITS);
-    std::vector<double> X(4096 * 2), Y(4096 * 2);
-    std::vector<double> tile_re(4096), tile_im(4096);
+    std::vector<double> X((size_t)ROWS * N), T(4096 * 2), O(4096 * 2);
+    std::vector<double> raw(4096 * 2);
     for (const FusedPass& P : plan.passes) {
+        if (P.n_blocks < 1 || P.n_blocks > fused_max_blocks(k)) return -5;
         for (uint64_t t = 0; t < tiles; t++) {
             uint64_t base = 0;
             for (int j = 0; j < P.n_nonlocal; j++) base |= ((t >> j) & 1ull) << P.nonlocal_q[j];
-            std::vector<int> seen(4096, 0);
-            for (uint32_t l = 0; l < 4096; l++) {
-                const uint64_t g = base + P.g_lo[l & 63] + P.g_hi[l >> 6];
-                const FusedBlock& B0 = plan.blocks[P.block_begin];
-                const uint32_t w = B0.off_lo[l & 63] + B0.off_hi[l >> 6];
-                if (w + 1 >= X.size() || seen[w / 2]++) return -2;
-                X[w] = re[g];
-                X[w + 1] = im[g];
+            // the raw tile: 256 runs of 16 amplitudes (local index 16 r + i)
+            for (uint32_t r = 0; r < 256; r++) {
+                const uint64_t g = base + P.g_lo[(r & 3) << 4] + P.g_hi[r >> 2];
+                for (uint32_t i = 0; i < 16; i++) {
+                    const uint32_t w = (16 * r + i) ^ ((uint32_t)P.raw_xor[r] << 1);
+                    raw[2 * w] = re[g + i];
+                    raw[2 * w + 1] = im[g + i];
+                }
+            }
+            const FusedBlock& B0 = plan.blocks[P.block_begin];
+            for (int nr = 0; nr < ROWS; nr++) {
+                const uint32_t rl = (uint32_t)B0.n_lo[nr & 31] ^ (uint32_t)B0.n_hi[nr >> 5];
+                for (int a = 0; a < A; a++) {
+                    const uint32_t l = rl ^ B0.a_sc[a];   // raw-tile word
+                    X[(size_t)nr * N + 2 * a] = raw[2 * l];
+                    X[(size_t)nr * N + 2 * a + 1] = raw[2 * l + 1];
+                }
             }
             for (int b = 0; b < P.n_blocks; b++) {
                 const FusedBlock& B = plan.blocks[P.block_begin + b];
-                const float* gh = plan.gates.data() + B.gate_word;
-                const float* gl = gh + (size_t)N * N;
-                for (int nrow = 0; nrow < ROWS; nrow++) {
+                const float* gop = plan.gates.data() + B.gate_word;
+                const bool last = (b + 1 == P.n_blocks);
+                std::vector<int> seen(4096, 0);
+                for (int nr = 0; nr < ROWS; nr++) {
                     std::vector<double> d(N, 0.0);
                     for (int mp = 0; mp < N; mp++) {
                         double s = 0;
                         for (int kk = 0; kk < N; kk++) {
-                            const uint32_t gw = emu_kmajor(mp, kk, N);
-                            s += X[emu_kmajor(nrow, kk, ROWS)] * ((double)gh[gw] + (double)gl[gw]);
+                            const double g = (double)gop[emu_kmajor(mp, kk, 2 * N)] +
+                                             (double)gop[emu_kmajor(N + mp, kk, 2 * N)];
+                            s += X[(size_t)nr * N + kk] * g;
                         }
                         d[mp] = s;
                     }
-                    // the kernel's scatter: additive next-offset tables
-                    const uint32_t wn = B.nxt_nlo[nrow & 31] + B.nxt_nhi[nrow >> 5];
-                    const uint32_t nl = B.n_lo[nrow & 31] | B.n_hi[nrow >> 5];
-                    for (int a = 0; a < (1 << k); a++) {
-                        const uint32_t w = wn + B.nxt_a[a];
-                        if (b + 1 < P.n_blocks) {
-                            const FusedBlock& B1 = plan.blocks[P.block_begin + b + 1];
-                            const uint32_t l = nl | B.a_sc[a];
-                            if (w != B1.off_lo[l & 63] + B1.off_hi[l >> 6]) return -4;
-                            Y[w] = d[2 * a];
-                            Y[w + 1] = d[2 * a + 1];
-                        } else {
-                            tile_re[w] = d[2 * a];
-                            tile_im[w] = d[2 * a + 1];
-                        }
+                    const uint32_t wn = (uint32_t)B.nxt_nlo[nr & 31] ^ (uint32_t)B.nxt_nhi[nr >> 5];
+                    for (int a = 0; a < A; a++) {
+                        const uint32_t w = wn ^ B.nxt_a[a];
+                        if (w >= 4096 || seen[w]++) return -2;
+                        std::vector<double>& dst = last ? O : T;
+                        dst[2 * w] = d[2 * a];
+                        dst[2 * w + 1] = d[2 * a + 1];
                     }
                 }
-                if (b + 1 < P.n_blocks) X.swap(Y);
+                if (!last) {
+                    // rows of the next block, read back at their transpose slots
+                    for (int nr = 0; nr < ROWS; nr++)
+                        for (int a = 0; a < A; a++) {
+                            const uint32_t w = fused_slot((uint32_t)nr, (uint32_t)a, k);
+                            X[(size_t)nr * N + 2 * a] = T[2 * w];
+                            X[(size_t)nr * N + 2 * a + 1] = T[2 * w + 1];
+                        }
+                }
             }
-            for (uint32_t l = 0; l < 4096; l++) {
-                const uint64_t g = base + P.g_lo[l & 63] + P.g_hi[l >> 6];
-                re[g] = tile_re[l];
-                im[g] = tile_im[l];
+            for (uint32_t r = 0; r < 256; r++) {
+                const uint64_t g = base + P.g_lo[(r & 3) << 4] + P.g_hi[r >> 2];
+                for (uint32_t i = 0; i < 16; i++) {
+                    const uint32_t w = (16 * r + i) ^ (uint32_t)P.out_xor[r];
+                    re[g + i] = O[2 * w];
+                    im[g + i] = O[2 * w + 1];
+                }
             }
         }
     }
@@ -410,5 +429,89 @@ extern "C" int emu_pairs_stats(uint32_t n, const svb_gate* gates, size_t n_gates
     stats[1] = plan.n_blocks;
     stats[2] = plan.n_swaps;
     stats[3] = plan.n_relayouts;
+    return 0;
+}
+
+// ---- shared-memory bank model of the fused kernel's accesses ---------------------------
+// Wavefronts of one warp access: 8-byte accesses go in two phases of 16 lanes (16 bank
+// pairs of 8 bytes), 16-byte accesses in four phases of 8 lanes (8 groups of 16 bytes);
+// within a phase, distinct words on the same bank unit serialise.
+static int emu_wavefronts(const uint32_t* word, int bytes)
+{
+    const int lanes = bytes == 8 ? 16 : 8, units = bytes == 8 ? 16 : 8;
+    int wf = 0;
+    for (int p = 0; p < 32 / lanes; p++) {
+        int worst = 0;
+        for (int u = 0; u < units; u++) {
+            uint32_t seen[32];
+            int cnt = 0;
+            for (int l = p * lanes; l < (p + 1) * lanes; l++) {
+                if ((int)(word[l] % (uint32_t)units) != u) continue;
+                bool dup = false;
+                for (int i = 0; i < cnt; i++) dup |= seen[i] == word[l];
+                if (!dup) seen[cnt++] = word[l];
+            }
+            if (cnt > worst) worst = cnt;
+        }
+        wf += worst;
+    }
+    return wf;
+}
+
+// Average wavefronts per warp instruction of the fused kernel's shared-memory accesses for
+// the plan of a circuit: out[0] block-0 gather from the raw tile (8-byte loads, ideal 2),
+// out[1] D rows into the transpose buffer (8-byte stores, ideal 2), out[2] rows read back
+// (16-byte loads, ideal 4), out[3] last block into the output stage (8-byte stores, ideal 2).
+extern "C" int emu_fused_conflicts(uint32_t n, const svb_gate* gates, size_t n_gates, int k, double* out)
+{
+    if ((int)n < FT_TILE_BITS || k < FT_MIN_K || k > FT_MAX_K) return -1;
+    std::vector<EOp> eops;
+    for (size_t i = 0; i < n_gates; i++)
+        if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
+    if (!fusable(eops)) return -3;
+    FusedPlan plan;
+    plan_fused(eops, (int)n, k, plan);
+    const int MBLK = (1 << (FT_TILE_BITS - k)) / 128, HALF = 1 << k, HAMP = HALF / 2;
+    double wf[4] = {0, 0, 0, 0}, ins[4] = {0, 0, 0, 0};
+    uint32_t word[32];
+    for (const FusedPass& P : plan.passes) {
+        for (int b = 0; b < P.n_blocks; b++) {
+            const FusedBlock& B = plan.blocks[P.block_begin + b];
+            const bool last = b + 1 == P.n_blocks;
+            for (int warp = 0; warp < FT_EPI_WARPS; warp++) {
+                const int quad = warp & 3, half = (warp >> 2) & 1;
+                for (int mb = 0; mb < MBLK; mb++)
+                    for (int a2 = 0; a2 < HAMP; a2++) {
+                        const int a = half * HAMP + a2;
+                        if (b == 0) {
+                            for (int lane = 0; lane < 32; lane++) {
+                                const uint32_t nr = (uint32_t)(128 * mb + 32 * quad + lane);
+                                word[lane] = (uint32_t)B.n_lo[nr & 31] ^ B.n_hi[nr >> 5] ^ B.a_sc[a];
+                            }
+                            wf[0] += emu_wavefronts(word, 8);
+                            ins[0] += 1;
+                        }
+                        for (int lane = 0; lane < 32; lane++) {
+                            const uint32_t nr = (uint32_t)(128 * mb + 32 * quad + lane);
+                            word[lane] = (uint32_t)B.nxt_nlo[nr & 31] ^ B.nxt_nhi[nr >> 5] ^ B.nxt_a[a];
+                        }
+                        wf[last ? 3 : 1] += emu_wavefronts(word, 8);
+                        ins[last ? 3 : 1] += 1;
+                    }
+                if (!last)
+                    for (int mb = 0; mb < MBLK; mb++)
+                        for (int c2 = 0; c2 < HAMP / 2; c2++) {
+                            const uint32_t c = (uint32_t)(half * (HAMP / 2) + c2);
+                            for (int lane = 0; lane < 32; lane++) {
+                                const uint32_t nr = (uint32_t)(128 * mb + 32 * quad + lane);
+                                word[lane] = fused_slot(nr, 2 * c, k) >> 1;
+                            }
+                            wf[2] += emu_wavefronts(word, 16);
+                            ins[2] += 1;
+                        }
+            }
+        }
+    }
+    for (int i = 0; i < 4; i++) out[i] = ins[i] > 0 ? wf[i] / ins[i] : 0.0;
     return 0;
 }

@@ -20,8 +20,10 @@ def run_fused(n, gates, k):
 
 
 @pytest.mark.parametrize("k", [3, 4, 5])
-@pytest.mark.parametrize("n", [12, 14, 17])
+@pytest.mark.parametrize("n", [12, 14, 17, 22])
 def test_fused_matches_oracle(oracle, n, k):
+    """n = 12..17 give each CTA one tile; n = 22 (1,024 tiles) gives each several, so both
+    tile slots, the prefetch buffers' reuse and the output stage's reuse run."""
     g = circuits.random_matching_circuit(n, 8, seed=100 * n + k)
     h = run_fused(n, g, k)
     re, im = h.get_state()
@@ -45,17 +47,18 @@ def test_fused_every_op(oracle):
                 "U1", "RX", "RY", "RZ", "CRX", "CRY", "CRZ", "CU1", "RXX", "RZZ", "RYY", "R") else 0)
             gl.append(G.FACTORIES[name](*([rng.uniform(-math.pi, math.pi) for _ in range(npar)] + qs)))
     g = G.to_array(gl)
-    h = run_fused(n, g, 5)
+    h = run_fused(n, g, 4)
     re, im = h.get_state()
     ore, oim = oracle.run(n, g)
     assert 1 - fidelity(re + 1j * im, ore + 1j * oim) <= 1e-6
 
 
-def test_fused_vs_fp64_on_device():
+@pytest.mark.parametrize("k", [4, 5])
+def test_fused_vs_fp64_on_device(k):
     from svsim_b200 import _native as nat
     n = 22
     g = circuits.random_matching_circuit(n, 10, seed=5)
-    h32 = run_fused(n, g, 5)
+    h32 = run_fused(n, g, k)
     h64 = nat.Handle(n, 0, nat.SVB_FP64)
     h64.set_circuit(g)
     h64.run()
@@ -82,7 +85,7 @@ def test_fused_run_keeps_unit_norm_and_small_amplitude_error():
     from svsim_b200 import _native as nat
     n = 20
     g = circuits.random_matching_circuit(n, 40, seed=9)
-    h32 = run_fused(n, g, 5)
+    h32 = run_fused(n, g, 4)
     assert abs(h32.norm2() - 1.0) <= 2e-6
     h64 = nat.Handle(n, 0, nat.SVB_FP64)
     h64.set_circuit(g)
