@@ -36,7 +36,7 @@ import numpy as np  # noqa: E402
 N_QUBITS = 30
 DEPTH = 40
 SEED = 2024
-FUSION_WIDTH = 4        # qubits per fused block of the tensor-core FP32 form
+FUSION_WIDTH = 5        # qubits per fused block of the tensor-core FP32 form
 METRIC = "n=30 gates/s & HBM GB/s: FP64 per-gate vs fused TC (1-F≤1e-6); adjoint grads/s"
 UNIT = "gates/s"
 WORKLOAD = "random circuit n=30 depth 40 (U3 all qubits + 15 CX random matching per layer), FP64"

@@ -6,12 +6,13 @@
 // block's real-form gate G[m'][kk] (N = 2^(k+1) square) is applied as
 //        D[n][m'] = sum_kk X[n][kk] G[m'][kk]
 // with tcgen05.mma.kind::tf32 (M = 128 rows per MMA, K = 8 per instruction) in three
-// products X_hi G_hi + X_hi G_lo + X_lo G_hi (split TF32: hi = x rounded to TF32, lo =
-// the remainder rounded to TF32), so the result keeps ~FP32 accuracy.  The gate operand
+// products X_hi G_hi + X_hi G_lo + X_lo G_hi (split TF32: hi = x as the MMA reads it,
+// i.e. truncated to TF32, lo = the remainder rounded to nearest TF32; the gate's halves
+// are split on the host from FP64), so the result keeps ~FP32 accuracy.  The gate operand
 // holds G_hi in rows 0..N-1 and G_lo in rows N..2N-1, so per K step one MMA of width 2N
 // forms [X_hi G_hi | X_hi G_lo] and one of width N adds X_lo G_hi to the first half.
 //
-// One persistent CTA per SM: 8 warps (two per TMEM lane quadrant) move the data and one
+// One persistent CTA per SM: 16 warps (four per TMEM lane quadrant) move the data and one
 // warp issues the MMAs.
 //  * The state operand (hi and lo planes) lives in tensor memory as the MMA's A operand;
 //    only the gate operand (B, canonical K-major layout, no swizzle) is read from shared
@@ -42,7 +43,8 @@ namespace {
 
 constexpr uint32_t kTmemCols = 512;      // two slots
 constexpr uint32_t kSlotCols = 256;
-constexpr uint32_t kWaitLimit = 1u << 26;
+constexpr uint32_t kSuspendNs = 20000;          // longest sleep of one mbarrier try
+constexpr uint64_t kWaitNs = 2000000000ull;     // a wait gives up after 2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -72,26 +74,45 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar)
                  :: "r"(smem_u32(bar)) : "memory");
 }
 
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// one try: the warp sleeps (issuing nothing) until the phase completes or kSuspendNs pass
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done) : "r"(a), "r"(parity), "r"(kSuspendNs) : "memory");
+    return done != 0;
+}
+
+// bounded wait: gives up after kWaitNs
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < kWaitLimit; it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done) : "r"(a), "r"(parity) : "memory");
-        if (done) return true;
-    }
+    if (mbar_try(a, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (global_ns() - t0 < kWaitNs)
+        if (mbar_try(a, parity)) return true;
     return false;
 }
 
-__device__ __forceinline__ float tf32_rna(float x)
+// x = hi + lo for the MMA: hi is x itself, of which the MMA reads only the top 19 bits
+// (x truncated to TF32), and lo is the exact remainder rounded to nearest TF32 (ties away
+// from zero: half a TF32 ulp added to the magnitude bits, then truncation), so no
+// truncation bias is left in the pair.
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo)
 {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    hi = x;
+    const float r = x - __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);   // exact
+    lo = __uint_as_float((__float_as_uint(r) + 0x1000u) & 0xFFFFE000u);
 }
 
 // 8 consecutive TMEM columns of this warp's 32 lanes
@@ -155,11 +176,30 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v)
         : "memory");
 }
 
-// W consecutive TMEM columns of this warp's 32 lanes (W = 8, 16 or 32)
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float* v)
+{
+    uint32_t r[4];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 4; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const float* v)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
+                 :: "r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])),
+                    "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3]))
+                 : "memory");
+}
+
+// W consecutive TMEM columns of this warp's 32 lanes (W = 4, 8, 16 or 32)
 template <int W>
 __device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, float* v)
 {
-    if constexpr (W == 8) {
+    if constexpr (W == 4) {
+        tmem_ld4(taddr, v);
+    } else if constexpr (W == 8) {
         tmem_ld8(taddr, v);
     } else {
 #pragma unroll
@@ -170,7 +210,9 @@ __device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, float* v)
 template <int W>
 __device__ __forceinline__ void tmem_st_cols(uint32_t taddr, const float* v)
 {
-    if constexpr (W == 8) {
+    if constexpr (W == 4) {
+        tmem_st4(taddr, v);
+    } else if constexpr (W == 8) {
         tmem_st8(taddr, v);
     } else {
 #pragma unroll
@@ -192,21 +234,17 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
 __device__ __forceinline__ bool mbar_wait_abort(uint64_t* bar, uint32_t parity, volatile int* abort)
 {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < kWaitLimit; it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done) : "r"(a), "r"(parity) : "memory");
-        if (done) return true;
-        if ((it & 31u) == 31u && *abort) return false;
+    if (mbar_try(a, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (global_ns() - t0 < kWaitNs) {
+        if (mbar_try(a, parity)) return true;
+        if (*abort) return false;
     }
     *abort = 1;
     return false;
 }
 
-// barrier of the 8 data warps (named barrier 1) that also ANDs a predicate over them
+// barrier of the data warps (named barrier 1) that also ANDs a predicate over them
 __device__ __forceinline__ bool epi_sync_and(bool p)
 {
     uint32_t r;
@@ -264,8 +302,10 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
     constexpr int ROWS = 1 << (FT_TILE_BITS - K);   // rows of the state operand
     constexpr int MBLK = ROWS / 128;                // M = 128 blocks
     constexpr int KSTEPS = N / 8;                   // tf32 MMA K = 8
-    constexpr int HALF = N / 2;                     // columns per thread and M block
-    constexpr int HAMP = HALF / 2;                  // amplitudes per thread and M block
+    constexpr int PARTS = FT_EPI_WARPS / 4;         // data warps per TMEM lane quadrant
+    constexpr int CW = N / PARTS;                   // columns per thread and M block
+    constexpr int CA = CW / 2;                      // amplitudes per thread and M block
+    constexpr int CHUNKS = 2048 / (FT_EPI_WARPS * 32);   // 16-byte chunks of a tile per thread
     constexpr int CPR = (1 << K) / 2;               // 16-byte chunks per transpose row
     constexpr int EPI = FT_EPI_WARPS * 32;          // data threads
     constexpr uint32_t GATE_WORDS = 2u * N * N;
@@ -274,7 +314,7 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
     using L = FusedSmem<K>;
     constexpr uint32_t NR = L::n_raw;
     static_assert(2 * PLANE + MBLK * DN <= kSlotCols && 2 * kSlotCols <= kTmemCols, "TMEM slots");
-    static_assert(HAMP % 2 == 0 && MBLK * HALF == 32 && EPI == 256, "thread share of a tile");
+    static_assert(CA % 2 == 0 && MBLK * CW * FT_EPI_WARPS == 256 && CHUNKS * EPI == 2048, "thread share of a tile");
 
     extern __shared__ __align__(128) unsigned char sm[];
     float2* trans = reinterpret_cast<float2*>(sm + L::trans);
@@ -295,7 +335,7 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
     const int warp = tid >> 5, lane = tid & 31;
     const bool mma_warp = warp == FT_EPI_WARPS;
     const int quad = warp & 3;          // TMEM lane quadrant of a data warp
-    const int half = (warp >> 2) & 1;   // which half of the columns it handles
+    const int part = warp >> 2;         // which part of the columns it handles
     const uint64_t my_tiles = blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     // -- stage the pass, its blocks and their gate operands in shared memory
@@ -416,38 +456,35 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
     } else if (run) {
         // ---- the data warps
         const uint32_t lane_base = (uint32_t)(quad * 32) << 16;
-        // the 8 16-byte chunks of a thread in a tile: chunk c = tid + 256 i is part tid & 7
-        // of run (tid >> 3) + 32 i (local index 16 run + 2 part)
+        // the 16-byte chunks of a thread in a tile: chunk c = tid + EPI i is piece tid & 7 of
+        // run (tid >> 3) + (EPI / 8) i (local index 16 run + 2 piece)
         const uint64_t g_part = P.g_lo[((tid >> 3) & 3) << 4] + 2u * (uint32_t)(tid & 7);
-        auto chunk_off = [&](int i) { return g_part + P.g_hi[(tid >> 5) + 8 * i]; };
+        auto chunk_off = [&](int i) { return g_part + P.g_hi[(tid >> 5) + (EPI / 32) * i]; };
 
-        // tile j into prefetch buffer j % NR (8 cp.async per thread, arriving on its mbarrier)
+        // tile j into prefetch buffer j % NR (CHUNKS cp.async per thread, arriving on its mbarrier)
         auto issue_load = [&](uint64_t j) {
             const uint32_t rb = (uint32_t)(j % NR);
             const float2* src = sv + tile_base(j);
             float2* dst = raw + rb * 4096u;
 #pragma unroll
-            for (int i = 0; i < 8; i++) {
+            for (int i = 0; i < CHUNKS; i++) {
                 const uint32_t c = (uint32_t)(tid + EPI * i);
                 cp_async16(dst + 2 * (c ^ P.raw_xor[c >> 3]), src + chunk_off(i));
             }
             cp_async_arrive(bar_load + rb);
             if (tid == 0) counts[4 + rb]++;
         };
-        // rows n = 128 mb + 32 quad + lane, columns half * HALF + [0, HALF): hi/lo into
+        // rows n = 128 mb + 32 quad + lane, columns part * CW + [0, CW): hi/lo into
         // the A planes of slot s, then this warp's arrival on the slot's ready barrier
-        auto put_rows = [&](int s, float (&v)[MBLK][HALF]) {
-            const uint32_t base = tmem + (uint32_t)s * kSlotCols + lane_base + (uint32_t)(half * HALF);
+        auto put_rows = [&](int s, float (&v)[MBLK][CW]) {
+            const uint32_t base = tmem + (uint32_t)s * kSlotCols + lane_base + (uint32_t)(part * CW);
 #pragma unroll
             for (int mb = 0; mb < MBLK; mb++) {
-                float h[HALF], l[HALF];
+                float h[CW], l[CW];
 #pragma unroll
-                for (int i = 0; i < HALF; i++) {
-                    h[i] = tf32_rna(v[mb][i]);
-                    l[i] = tf32_rna(v[mb][i] - h[i]);
-                }
-                tmem_st_cols<HALF>(base + (uint32_t)(mb * N), h);
-                tmem_st_cols<HALF>(base + PLANE + (uint32_t)(mb * N), l);
+                for (int i = 0; i < CW; i++) split_tf32(v[mb][i], h[i], l[i]);
+                tmem_st_cols<CW>(base + (uint32_t)(mb * N), h);
+                tmem_st_cols<CW>(base + PLANE + (uint32_t)(mb * N), l);
             }
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -467,23 +504,23 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
             const bool got = mbar_wait_abort(bar_load + rb, (uint32_t)((j / NR) & 1u), abort_flag);
             const float2* R = raw + rb * 4096u;
             const FusedBlock& B0 = sb[0];
-            float v[MBLK][HALF];
+            float v[MBLK][CW];
 #pragma unroll
             for (int mb = 0; mb < MBLK; mb++) {
                 const uint32_t n = (uint32_t)(128 * mb + 32 * quad + lane);
                 const uint32_t rl = (uint32_t)B0.n_lo[n & 31u] ^ (uint32_t)B0.n_hi[n >> 5];
 #pragma unroll
-                for (int a2 = 0; a2 < HAMP; a2++) {
-                    const float2 x = R[rl ^ (uint32_t)B0.a_sc[half * HAMP + a2]];
+                for (int a2 = 0; a2 < CA; a2++) {
+                    const float2 x = R[rl ^ (uint32_t)B0.a_sc[part * CA + a2]];
                     v[mb][2 * a2] = x.x;
                     v[mb][2 * a2 + 1] = x.y;
                 }
             }
+            put_rows(s, v);
             // every thread's reads of the buffer are done before it is refilled
             if (!epi_sync_and(got)) return false;
             if (tid == 0) counts[6 + rb]++;
             if (j + NR < my_tiles) issue_load(j + NR);
-            put_rows(s, v);
             return true;
         };
 
@@ -492,19 +529,19 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
             if (!act || !ok) return;
             const bool got = mbar_wait_abort(bar_mma + s, mpar, abort_flag);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            float v[MBLK][HALF], w[MBLK][HALF];
-            const uint32_t dcol = tmem + (uint32_t)s * kSlotCols + lane_base + 2u * PLANE + (uint32_t)(half * HALF);
+            float v[MBLK][CW], w[MBLK][CW];
+            const uint32_t dcol = tmem + (uint32_t)s * kSlotCols + lane_base + 2u * PLANE + (uint32_t)(part * CW);
 #pragma unroll
             for (int mb = 0; mb < MBLK; mb++) {
-                tmem_ld_cols<HALF>(dcol + (uint32_t)(mb * DN), v[mb]);
-                tmem_ld_cols<HALF>(dcol + (uint32_t)(mb * DN + N), w[mb]);
+                tmem_ld_cols<CW>(dcol + (uint32_t)(mb * DN), v[mb]);
+                tmem_ld_cols<CW>(dcol + (uint32_t)(mb * DN + N), w[mb]);
             }
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 #pragma unroll
             for (int mb = 0; mb < MBLK; mb++)
 #pragma unroll
-                for (int i = 0; i < HALF; i++) v[mb][i] += w[mb][i];
+                for (int i = 0; i < CW; i++) v[mb][i] += w[mb][i];
             const FusedBlock& B = sb[blk];
             float2* T = trans + tsel * 4096u;
             tsel ^= 1u;
@@ -515,8 +552,8 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
                 const uint32_t n = (uint32_t)(128 * mb + 32 * quad + lane);
                 const uint32_t wn = (uint32_t)B.nxt_nlo[n & 31u] ^ (uint32_t)B.nxt_nhi[n >> 5];
 #pragma unroll
-                for (int a2 = 0; a2 < HAMP; a2++)
-                    T[wn ^ (uint32_t)B.nxt_a[half * HAMP + a2]] = make_float2(v[mb][2 * a2], v[mb][2 * a2 + 1]);
+                for (int a2 = 0; a2 < CA; a2++)
+                    T[wn ^ (uint32_t)B.nxt_a[part * CA + a2]] = make_float2(v[mb][2 * a2], v[mb][2 * a2 + 1]);
             }
             if (!epi_sync_and(got)) { ok = false; return; }
             mpar ^= 1u;
@@ -529,8 +566,8 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
                     const uint32_t n = (uint32_t)(128 * mb + 32 * quad + lane);
                     const bool swap = (n >> 3) & 1u;       // fused_slot swaps a chunk's amplitudes
 #pragma unroll
-                    for (int c2 = 0; c2 < HAMP / 2; c2++) {
-                        const uint32_t c = (uint32_t)(half * (HAMP / 2) + c2);
+                    for (int c2 = 0; c2 < CA / 2; c2++) {
+                        const uint32_t c = (uint32_t)(part * (CA / 2) + c2);
                         const float4 x = t4[n * CPR + (c ^ fused_chunk_swizzle(n, K))];
                         v[mb][4 * c2] = swap ? x.z : x.x;
                         v[mb][4 * c2 + 1] = swap ? x.w : x.y;
@@ -544,7 +581,7 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
                 // the tile out in 16-byte pieces (8 threads per 128-byte run)
                 float2* dst = sv + tile_base(tj);
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
+                for (int i = 0; i < CHUNKS; i++) {
                     const uint32_t c = (uint32_t)(tid + EPI * i);
                     const uint32_t ox = P.out_xor[c >> 3];
                     float4 x = t4[c ^ (ox >> 1)];

@@ -205,7 +205,7 @@ constexpr int FT_MAX_BLOCKS = 8;     // upper bound of fused blocks per pass
 // two buffers and 5 (k = 4) or 8 (k = 3) blocks, all inside the 227 KiB of one CTA.
 __host__ __device__ constexpr int fused_max_blocks(int k) { return k >= 5 ? 3 : (k == 4 ? 5 : 8); }
 __host__ __device__ constexpr int fused_raw_buffers(int k) { return k >= 5 ? 1 : 2; }
-constexpr int FT_EPI_WARPS = 8;      // warps that move tiles and operands: two per TMEM lane quadrant
+constexpr int FT_EPI_WARPS = 16;     // warps that move tiles and operands: four per TMEM lane quadrant
 constexpr int FT_THREADS = 32 * (FT_EPI_WARPS + 1);   // plus one warp that issues the MMAs
 constexpr int FT_MAX_NONLOCAL = 24;  // tile-index bits of a pass (n <= 36)
 constexpr int FT_MIN_K = 3, FT_MAX_K = 5;

@@ -471,7 +471,8 @@ extern "C" int emu_fused_conflicts(uint32_t n, const svb_gate* gates, size_t n_g
     if (!fusable(eops)) return -3;
     FusedPlan plan;
     plan_fused(eops, (int)n, k, plan);
-    const int MBLK = (1 << (FT_TILE_BITS - k)) / 128, HALF = 1 << k, HAMP = HALF / 2;
+    const int PARTS = FT_EPI_WARPS / 4;
+    const int MBLK = (1 << (FT_TILE_BITS - k)) / 128, CW = (2 << k) / PARTS, CA = CW / 2;
     double wf[4] = {0, 0, 0, 0}, ins[4] = {0, 0, 0, 0};
     uint32_t word[32];
     for (const FusedPass& P : plan.passes) {
@@ -479,10 +480,10 @@ extern "C" int emu_fused_conflicts(uint32_t n, const svb_gate* gates, size_t n_g
             const FusedBlock& B = plan.blocks[P.block_begin + b];
             const bool last = b + 1 == P.n_blocks;
             for (int warp = 0; warp < FT_EPI_WARPS; warp++) {
-                const int quad = warp & 3, half = (warp >> 2) & 1;
+                const int quad = warp & 3, part = warp >> 2;
                 for (int mb = 0; mb < MBLK; mb++)
-                    for (int a2 = 0; a2 < HAMP; a2++) {
-                        const int a = half * HAMP + a2;
+                    for (int a2 = 0; a2 < CA; a2++) {
+                        const int a = part * CA + a2;
                         if (b == 0) {
                             for (int lane = 0; lane < 32; lane++) {
                                 const uint32_t nr = (uint32_t)(128 * mb + 32 * quad + lane);
@@ -500,8 +501,8 @@ extern "C" int emu_fused_conflicts(uint32_t n, const svb_gate* gates, size_t n_g
                     }
                 if (!last)
                     for (int mb = 0; mb < MBLK; mb++)
-                        for (int c2 = 0; c2 < HAMP / 2; c2++) {
-                            const uint32_t c = (uint32_t)(half * (HAMP / 2) + c2);
+                        for (int c2 = 0; c2 < CA / 2; c2++) {
+                            const uint32_t c = (uint32_t)(part * (CA / 2) + c2);
                             for (int lane = 0; lane < 32; lane++) {
                                 const uint32_t nr = (uint32_t)(128 * mb + 32 * quad + lane);
                                 word[lane] = fused_slot(nr, 2 * c, k) >> 1;
