@@ -257,6 +257,24 @@ __device__ __forceinline__ bool epi_sync_and(bool p)
     return r != 0;
 }
 
+// CA consecutive 16-bit table entries (CA = 2, 4 or 8; 4-byte aligned) in one load
+template <int CA>
+__device__ __forceinline__ void load_u16(const uint16_t* t, uint32_t* out)
+{
+    if constexpr (CA == 8) {
+        const uint4 q = *reinterpret_cast<const uint4*>(t);
+        const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int i = 0; i < 4; i++) { out[2 * i] = w[i] & 0xFFFFu; out[2 * i + 1] = w[i] >> 16; }
+    } else if constexpr (CA == 4) {
+        const uint2 q = *reinterpret_cast<const uint2*>(t);
+        out[0] = q.x & 0xFFFFu; out[1] = q.x >> 16; out[2] = q.y & 0xFFFFu; out[3] = q.y >> 16;
+    } else {
+        const uint32_t q = *reinterpret_cast<const uint32_t*>(t);
+        out[0] = q & 0xFFFFu; out[1] = q >> 16;
+    }
+}
+
 // 16 bytes global -> shared, asynchronous (L2 only)
 __device__ __forceinline__ void cp_async16(void* dst, const void* src)
 {
@@ -458,8 +476,21 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
         const uint32_t lane_base = (uint32_t)(quad * 32) << 16;
         // the 16-byte chunks of a thread in a tile: chunk c = tid + EPI i is piece tid & 7 of
         // run (tid >> 3) + (EPI / 8) i (local index 16 run + 2 piece)
-        const uint64_t g_part = P.g_lo[((tid >> 3) & 3) << 4] + 2u * (uint32_t)(tid & 7);
-        auto chunk_off = [&](int i) { return g_part + P.g_hi[(tid >> 5) + (EPI / 32) * i]; };
+        // Fixed for the pass: their global offsets within a tile, their slots in a raw
+        // tile and where they sit in the output stage (with the swap of its two halves).
+        uint64_t goff[CHUNKS];
+        uint32_t rslot[CHUNKS], oslot[CHUNKS];
+        {
+            const uint64_t g_part = P.g_lo[((tid >> 3) & 3) << 4] + 2u * (uint32_t)(tid & 7);
+#pragma unroll
+            for (int i = 0; i < CHUNKS; i++) {
+                const uint32_t c = (uint32_t)(tid + EPI * i);
+                goff[i] = g_part + P.g_hi[(tid >> 5) + (EPI / 32) * i];
+                rslot[i] = c ^ P.raw_xor[c >> 3];
+                const uint32_t ox = P.out_xor[c >> 3];
+                oslot[i] = ((c ^ (ox >> 1)) << 1) | (ox & 1u);
+            }
+        }
 
         // tile j into prefetch buffer j % NR (CHUNKS cp.async per thread, arriving on its mbarrier)
         auto issue_load = [&](uint64_t j) {
@@ -467,10 +498,7 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
             const float2* src = sv + tile_base(j);
             float2* dst = raw + rb * 4096u;
 #pragma unroll
-            for (int i = 0; i < CHUNKS; i++) {
-                const uint32_t c = (uint32_t)(tid + EPI * i);
-                cp_async16(dst + 2 * (c ^ P.raw_xor[c >> 3]), src + chunk_off(i));
-            }
+            for (int i = 0; i < CHUNKS; i++) cp_async16(dst + 2 * rslot[i], src + goff[i]);
             cp_async_arrive(bar_load + rb);
             if (tid == 0) counts[4 + rb]++;
         };
@@ -504,6 +532,8 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
             const bool got = mbar_wait_abort(bar_load + rb, (uint32_t)((j / NR) & 1u), abort_flag);
             const float2* R = raw + rb * 4096u;
             const FusedBlock& B0 = sb[0];
+            uint32_t asc[CA];
+            load_u16<CA>(B0.a_sc + part * CA, asc);
             float v[MBLK][CW];
 #pragma unroll
             for (int mb = 0; mb < MBLK; mb++) {
@@ -511,7 +541,7 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
                 const uint32_t rl = (uint32_t)B0.n_lo[n & 31u] ^ (uint32_t)B0.n_hi[n >> 5];
 #pragma unroll
                 for (int a2 = 0; a2 < CA; a2++) {
-                    const float2 x = R[rl ^ (uint32_t)B0.a_sc[part * CA + a2]];
+                    const float2 x = R[rl ^ asc[a2]];
                     v[mb][2 * a2] = x.x;
                     v[mb][2 * a2 + 1] = x.y;
                 }
@@ -543,6 +573,8 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
 #pragma unroll
                 for (int i = 0; i < CW; i++) v[mb][i] += w[mb][i];
             const FusedBlock& B = sb[blk];
+            uint32_t na[CA];
+            load_u16<CA>(B.nxt_a + part * CA, na);
             float2* T = trans + tsel * 4096u;
             tsel ^= 1u;
             // D rows into the transpose buffer: the next block's row order, or (last block)
@@ -553,7 +585,7 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
                 const uint32_t wn = (uint32_t)B.nxt_nlo[n & 31u] ^ (uint32_t)B.nxt_nhi[n >> 5];
 #pragma unroll
                 for (int a2 = 0; a2 < CA; a2++)
-                    T[wn ^ (uint32_t)B.nxt_a[part * CA + a2]] = make_float2(v[mb][2 * a2], v[mb][2 * a2 + 1]);
+                    T[wn ^ na[a2]] = make_float2(v[mb][2 * a2], v[mb][2 * a2 + 1]);
             }
             if (!epi_sync_and(got)) { ok = false; return; }
             mpar ^= 1u;
@@ -582,11 +614,9 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
                 float2* dst = sv + tile_base(tj);
 #pragma unroll
                 for (int i = 0; i < CHUNKS; i++) {
-                    const uint32_t c = (uint32_t)(tid + EPI * i);
-                    const uint32_t ox = P.out_xor[c >> 3];
-                    float4 x = t4[c ^ (ox >> 1)];
-                    if (ox & 1u) x = make_float4(x.z, x.w, x.x, x.y);
-                    *reinterpret_cast<float4*>(dst + chunk_off(i)) = x;
+                    float4 x = t4[oslot[i] >> 1];
+                    if (oslot[i] & 1u) x = make_float4(x.z, x.w, x.x, x.y);
+                    *reinterpret_cast<float4*>(dst + goff[i]) = x;
                 }
                 if (next_j < my_tiles) {
                     tj = next_j++;
