@@ -365,7 +365,8 @@ def fused_form(device, circuit, k=None, reps=3, n=N_QUBITS):
            "hbm_frac_of_peak": info.moved_bytes / s / 1e9 / peak,
            "one_minus_fidelity_vs_fp64": 1.0 - fid, "max_abs_amp_err_vs_fp64": maxd,
            "norm_minus_one": norm32 - 1.0,
-           "kernel": f"k_fused<{k}>: split-TF32 tcgen05.mma (M=128, N=K={2 << k}), A operand and "
+           "kernel": f"k_fused<{k}>: split-TF32 tcgen05.mma, M=128, K={2 << k} in steps of 8, "
+                     f"N={4 << k} (X_hi [G_hi|G_lo]) + N={2 << k} (X_lo G_hi); A operand and "
                      "accumulators in TMEM, two tiles in flight"}
     del h32
     torch.cuda.empty_cache()
