@@ -513,6 +513,7 @@ svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* g
         if (!R.gates.empty())
             SVB_CUDA(cudaMemcpy(s->dpairs.gates, R.gates.data(), R.gates.size() * sizeof(double),
                                 cudaMemcpyHostToDevice), "plan upload");
+        s->dpairs.stage_bytes = R.stage_bytes;
         s->info.n_passes = R.passes.size();
         s->info.tile_bits = PR_TILE_BITS;
         s->info.plan_bytes = R.passes.size() * sizeof(PairPass) + R.ops.size() * sizeof(PairOp) +

@@ -93,19 +93,13 @@ __device__ __forceinline__ uint64_t pair_goff(const PairGOffs& g, int k)
     return r;
 }
 
-__device__ __forceinline__ PairOp load_op(const PairOp* p)
-{
-    const uint4 w = __ldg(reinterpret_cast<const uint4*>(p));
-    PairOp o;
-    *reinterpret_cast<uint4*>(&o) = w;
-    return o;
-}
-
 __global__ void __launch_bounds__(PR_THREADS, 2)
 k_pairs(double2* __restrict__ sv, const PairPass* __restrict__ passes, const PairOp* __restrict__ ops,
         const DevStage* __restrict__ layouts, const double2* __restrict__ gates, int pass_index,
         uint64_t tiles)
 {
+    // shared memory: the tile, then the pass's ops, layouts and (when they fit) gates,
+    // copied once per CTA so that the op loop reads no global memory but the tile
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2* sm = reinterpret_cast<double2*>(smem_raw);
     __shared__ PairPass sP;
@@ -118,10 +112,27 @@ k_pairs(double2* __restrict__ sv, const PairPass* __restrict__ passes, const Pai
         __syncthreads();
     }
     const PairPass& P = sP;
-    const int ob = P.op_begin, oe = P.op_end;
+    const int n_ops = P.op_end - P.op_begin;
+    const int n_lay = P.store_layout - P.load_layout + 1;
+    PairOp* sops = reinterpret_cast<PairOp*>(smem_raw + (sizeof(double2) << PR_TILE_BITS));
+    DevStage* slay = reinterpret_cast<DevStage*>(reinterpret_cast<unsigned char*>(sops) + 16 * (size_t)n_ops);
+    double2* sg = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(slay) +
+                                             ((24 * (size_t)n_lay + 15) / 16) * 16);
+    {
+        const uint4* o4 = reinterpret_cast<const uint4*>(ops + P.op_begin);
+        for (int w = tid; w < n_ops; w += PR_THREADS) reinterpret_cast<uint4*>(sops)[w] = o4[w];
+        const uint32_t* l4 = reinterpret_cast<const uint32_t*>(layouts + P.load_layout);
+        for (int w = tid; w < n_lay * 6; w += PR_THREADS) reinterpret_cast<uint32_t*>(slay)[w] = l4[w];
+        if (P.stage_gates) {
+            const double2* g = gates + (size_t)P.gate_begin * 32;
+            for (int w = tid; w < P.gate_count * 32; w += PR_THREADS) sg[w] = g[w];
+        }
+        __syncthreads();
+    }
+    const double2* G = P.stage_gates ? sg : gates + (size_t)P.gate_begin * 32;
     PairGOffs gin, gout;
-    pair_goffs(layouts[P.load_layout], P.local_q, tid, gin);
-    pair_goffs(layouts[P.store_layout], P.local_q, tid, gout);
+    pair_goffs(slay[0], P.local_q, tid, gin);
+    pair_goffs(slay[n_lay - 1], P.local_q, tid, gout);
 
     for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         uint64_t base = 0;
@@ -129,12 +140,14 @@ k_pairs(double2* __restrict__ sv, const PairPass* __restrict__ passes, const Pai
         double2 v[PR_NR];
 #pragma unroll
         for (int k = 0; k < PR_NR; k++) v[k] = sv[base | pair_goff(gin, k)];
-        for (int o = ob; o < oe; o++) {
-            const PairOp op = load_op(ops + o);
+        for (int o = 0; o < n_ops; o++) {
+            const PairOp op = sops[o];
             if (op.kind == PO_BLOCK) {
+                static_assert(PR_MAX_COND == 2, "condition qubits of a block");
                 int var = 0;
-                for (int c = 0; c < op.ncond; c++) var |= (int)((base >> op.cond_q[c]) & 1ull) << c;
-                const double2 g = __ldg(gates + (size_t)(op.gate + var) * 32 + lane);
+                if (op.ncond > 0) var |= (int)((base >> op.cond_q[0]) & 1ull);
+                if (op.ncond > 1) var |= (int)((base >> op.cond_q[1]) & 1ull) << 1;
+                const double2 g = G[(size_t)((int)op.gate - P.gate_begin + var) * 32 + lane];
 #pragma unroll
                 for (int k = 0; k < PR_NR; k++) {
                     double d0, d1;
@@ -147,8 +160,8 @@ k_pairs(double2* __restrict__ sv, const PairPass* __restrict__ passes, const Pai
                 swap_any(v, op.lane, op.reg);
             } else {
                 Slots from, to;
-                make_slots<double, PR_TILE_BITS - RB>(layouts[op.src], tid, from);
-                make_slots<double, PR_TILE_BITS - RB>(layouts[op.layout], tid, to);
+                make_slots<double, PR_TILE_BITS - RB>(slay[op.src - P.load_layout], tid, from);
+                make_slots<double, PR_TILE_BITS - RB>(slay[op.layout - P.load_layout], tid, to);
 #pragma unroll
                 for (int k = 0; k < PR_NR; k++) sm[slot_of(from, k)] = v[k];
                 __syncthreads();
@@ -169,12 +182,13 @@ cudaError_t launch_pair_pass(void* state, int n, int pass_index, const DevPairBu
     static int max_ctas[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
-    const size_t smem = sizeof(double2) << PR_TILE_BITS;
+    const size_t smem = (sizeof(double2) << PR_TILE_BITS) + b.stage_bytes;
+    if (smem > PR_SMEM_CAP) return cudaErrorInvalidValue;
     if (dev < 64 && max_ctas[dev] == 0) {
-        cudaError_t e = cudaFuncSetAttribute(k_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PR_SMEM_CAP);
         if (e != cudaSuccess) return e;
         int per_sm = 0, sms = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs, PR_THREADS, smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs, PR_THREADS, PR_SMEM_CAP);
         if (e != cudaSuccess) return e;
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;

@@ -483,6 +483,7 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
         lp.set(sp);
         P.load_layout = lp.push_layout();
         P.op_begin = (int32_t)plan.ops.size();
+        P.gate_begin = (int32_t)(plan.gates.size() / 64);
         // blocks on disjoint pairs commute: take them in an order that needs few moves.
         // Block j may go once every earlier block sharing a qubit with it has gone.
         std::vector<int> order;
@@ -554,6 +555,14 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
         }
         P.store_layout = lp.push_layout();
         P.op_end = (int32_t)plan.ops.size();
+        P.gate_count = (int32_t)(plan.gates.size() / 64) - P.gate_begin;
+        // what the kernel copies into shared memory beside the tile
+        const size_t tile = sizeof(double) * 2 << PR_TILE_BITS;
+        const size_t fixed = pair_stage_bytes(P.op_end - P.op_begin, P.store_layout - P.load_layout + 1, 0);
+        const size_t with_gates = pair_stage_bytes(P.op_end - P.op_begin, P.store_layout - P.load_layout + 1,
+                                                   P.gate_count);
+        P.stage_gates = tile + with_gates <= PR_SMEM_CAP ? 1 : 0;
+        plan.stage_bytes = std::max(plan.stage_bytes, P.stage_gates ? with_gates : fixed);
         plan.passes.push_back(P);
         return std::vector<int>{};
     });

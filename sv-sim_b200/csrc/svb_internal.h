@@ -158,9 +158,19 @@ struct PairPass {
     uint8_t nonlocal_q[64 - PR_TILE_BITS];
     int32_t n_nonlocal;
     int32_t op_begin, op_end;
-    int32_t load_layout, store_layout;
-    int32_t pad;
+    int32_t load_layout, store_layout;   // the pass's layouts are load_layout..store_layout
+    int32_t gate_begin, gate_count;      // its blocks' gate fragments (32 lanes x 16 bytes)
+    int32_t stage_gates;                 // whether they are copied into shared memory too
 };
+static_assert(sizeof(PairPass) % 16 == 0, "PairPass layout");
+// Shared memory of a pair CTA: the 64 KiB tile, then the pass's ops, layouts and (when
+// they fit) gate fragments, all within what two CTAs per SM can hold.
+constexpr size_t PR_SMEM_CAP = 112 * 1024;
+// bytes of a pass's ops, layouts and gate fragments in shared memory (16-byte aligned parts)
+inline size_t pair_stage_bytes(int n_ops, int n_layouts, int n_gates)
+{
+    return 16 * (size_t)n_ops + ((24 * (size_t)n_layouts + 15) / 16) * 16 + 512 * (size_t)n_gates;
+}
 
 struct PairPlan {
     std::vector<PairPass> passes;
@@ -168,6 +178,7 @@ struct PairPlan {
     std::vector<DevStage> layouts;
     std::vector<double> gates;           // per variant: 32 lanes x (B0, B1)
     size_t n_blocks = 0, n_swaps = 0, n_relayouts = 0;
+    size_t stage_bytes = 0;              // largest per-pass copy into shared memory
 };
 
 // 4x4 complex matrix of an F_M4 op, row-major, re/im interleaved (index a = bit0 + 2 bit1)
@@ -182,6 +193,7 @@ struct DevPairBuffers {
     PairOp* ops = nullptr;
     DevStage* layouts = nullptr;
     double* gates = nullptr;
+    size_t stage_bytes = 0;
 };
 cudaError_t launch_pair_pass(void* state, int n, int pass_index, const DevPairBuffers& b, cudaStream_t s);
 
