@@ -22,7 +22,7 @@ constexpr int PR_NR = 1 << RB;                          // 16
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b, double c0, double c1)
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};"
                  : "=d"(d0), "=d"(d1)
                  : "d"(a), "d"(b), "d"(c0), "d"(c1));
 }
