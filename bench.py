@@ -276,6 +276,16 @@ def run_ours(args):
                 "peak_source": f"{peak_kind} hbm_gbs",
                 "per_launch_bytes": per_launch_bytes, "launches_per_step": passes,
                 "gate_model_gbs": info.model_bytes / (ms_per_step / 1e3) / 1e9}
+    if args.engine == "pairs" and int(info.n_blocks) > 0:
+        # the pair kernel is bound by the FP64 tensor cores, not by HBM: each two-qubit
+        # block is 16 multiply-adds per amplitude; the rate they allow is measured live
+        flops = int(info.n_blocks) * float(1 << nq) * 16 * 2
+        tf = flops / (ms_per_step / 1e3) / 1e12
+        tf_peak = nat.fp64_mma_peak(device)
+        roofline["fp64_tensor"] = {"achieved": tf, "peak": tf_peak, "unit": "TFLOP/s", "frac": tf / tf_peak,
+                                   "blocks_per_step": int(info.n_blocks),
+                                   "peak_source": "svb_fp64_mma_peak: register-only mma.sync m8n8k4 f64 loop, "
+                                                  "measured in this run"}
 
     # end to end through the C ABI with host buffers: circuit upload + plan, run,
     # 1024-shot measurement back to host

@@ -90,6 +90,8 @@ typedef struct svb_plan_info {
     uint64_t plan_bytes;       /* bytes of plan descriptors uploaded by svb_set_circuit */
     int      engine;           /* engine the plan was built for */
     int      tile_bits;        /* local qubits per tile (staged engine) */
+    uint64_t n_blocks;         /* tensor-core blocks per run: two-qubit blocks of the pair
+                                  engine, fused blocks of the fused engine; 0 otherwise */
 } svb_plan_info;
 
 typedef struct svb_sim svb_sim;
@@ -292,6 +294,11 @@ const char* svb_last_error(void);
 
 /* Library version string. */
 const char* svb_version(void);
+
+/* No reference counterpart (a measurement helper): times a register-only loop of FP64
+ * tensor-core MMAs (mma.sync m8n8k4 f64, 8 independent chains per warp) on `device` for a
+ * few milliseconds and writes the rate in TFLOP/s: the bound of the pair engine's blocks. */
+svb_status svb_fp64_mma_peak(int device, double* tflops);
 
 #ifdef __cplusplus
 }

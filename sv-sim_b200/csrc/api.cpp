@@ -484,6 +484,7 @@ svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* g
                                 cudaMemcpyHostToDevice), "plan upload");
         s->info.n_passes = F.passes.size();
         s->info.tile_bits = FT_TILE_BITS;
+        s->info.n_blocks = F.blocks.size();
         s->info.plan_bytes = F.passes.size() * sizeof(FusedPass) + F.blocks.size() * sizeof(FusedBlock) +
                              F.gates.size() * sizeof(float);
         // one read + write per pass, then the renormalisation (two reads, one write)
@@ -516,6 +517,7 @@ svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* g
         s->dpairs.stage_bytes = R.stage_bytes;
         s->info.n_passes = R.passes.size();
         s->info.tile_bits = PR_TILE_BITS;
+        s->info.n_blocks = R.n_blocks;
         s->info.plan_bytes = R.passes.size() * sizeof(PairPass) + R.ops.size() * sizeof(PairOp) +
                              R.layouts.size() * sizeof(DevStage) + R.gates.size() * sizeof(double);
         s->info.moved_bytes = 2.0 * sb * (double)R.passes.size();

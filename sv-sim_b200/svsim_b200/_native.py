@@ -32,7 +32,7 @@ class PlanInfo(ctypes.Structure):
                 ("state_bytes", ctypes.c_double), ("model_bytes", ctypes.c_double),
                 ("moved_bytes", ctypes.c_double), ("plan_bytes", ctypes.c_uint64),
                 ("engine", ctypes.c_int),
-                ("tile_bits", ctypes.c_int)]
+                ("tile_bits", ctypes.c_int), ("n_blocks", ctypes.c_uint64)]
 
 
 class QaoaStats(ctypes.Structure):
@@ -82,6 +82,7 @@ _SIGS = {
     "svb_dm_probabilities": ([_vp, _dp], ctypes.c_int),
     "svb_last_error": ([], ctypes.c_char_p),
     "svb_version": ([], ctypes.c_char_p),
+    "svb_fp64_mma_peak": ([ctypes.c_int, _dp], ctypes.c_int),
 }
 
 
@@ -108,6 +109,13 @@ def check(status: int):
 
 def dptr(a: np.ndarray):
     return a.ctypes.data_as(_dp)
+
+
+def fp64_mma_peak(device: int = 0) -> float:
+    """FP64 tensor-core rate in TFLOP/s measured on `device` (svb_fp64_mma_peak)."""
+    v = ctypes.c_double()
+    check(lib().svb_fp64_mma_peak(device, ctypes.byref(v)))
+    return v.value
 
 
 class Handle:
