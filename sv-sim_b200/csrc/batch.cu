@@ -74,8 +74,9 @@ struct QaoaArgs {
     void* lam;
     const void* cost;            // C(z): double for FP64 batches, float for FP32
     const QaoaDesc* inst;
+    const uint32_t* item_inst;   // [item]: the instance a tile belongs to
     const double* gammas;        // [inst][p]
-    const double* betas;         // [inst][p]
+    const double* mix;           // [inst][p] x (cos beta, -sin beta), from the host
     double* partial;             // [item][1 + 3p]: energy, dgamma_l, dbeta_l (low), dbeta_l (high)
     double* energy;              // [inst]
     double* grad;                // [inst][2p]: dE/dgamma_0..p-1, dE/dbeta_0..p-1
@@ -116,6 +117,29 @@ __device__ __forceinline__ void grid_barrier(unsigned* bar, unsigned target)
         __threadfence();
     }
     __syncthreads();
+}
+
+// two block sums in one pass (red holds 2 * QB_THREADS / 32 doubles); thread 0 gets both
+__device__ __forceinline__ void block_sum2(double v, double w, double* red, double& sv, double& sw)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+        w += __shfl_xor_sync(0xffffffffu, w, o);
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+        red[threadIdx.x >> 5] = v;
+        red[QB_THREADS / 32 + (threadIdx.x >> 5)] = w;
+    }
+    __syncthreads();
+    sv = 0;
+    sw = 0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < QB_THREADS / 32; i++) {
+            sv += red[i];
+            sw += red[QB_THREADS / 32 + i];
+        }
 }
 
 __device__ __forceinline__ double block_sum(double v, double* red)
@@ -241,6 +265,28 @@ __device__ __forceinline__ void exchange(typename AmpOf<T>::type* r, typename Am
     for (int k = 0; k < C::NR; k++) r[k] = buf[swz<T>(tb_to | reg_off<T, ST>(k))];
 }
 
+// psi and lambda through their two buffers behind one barrier
+template <typename T, int SF, int ST>
+__device__ __forceinline__ void exchange2(typename AmpOf<T>::type* p, typename AmpOf<T>::type* l,
+                                          typename AmpOf<T>::type* bp, typename AmpOf<T>::type* bl,
+                                          uint32_t tb_from, uint32_t tb_to)
+{
+    using C = QbCfg<T>;
+#pragma unroll
+    for (int k = 0; k < C::NR; k++) {
+        const uint32_t a = swz<T>(tb_from | reg_off<T, SF>(k));
+        bp[a] = p[k];
+        bl[a] = l[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < C::NR; k++) {
+        const uint32_t a = swz<T>(tb_to | reg_off<T, ST>(k));
+        p[k] = bp[a];
+        l[k] = bl[a];
+    }
+}
+
 __device__ __forceinline__ void cis(double ang, double& cr, double& ci) { sincos(ang, &ci, &cr); }
 __device__ __forceinline__ void cis(float ang, float& cr, float& ci) { sincosf(ang, &ci, &cr); }
 
@@ -280,11 +326,7 @@ __global__ void __launch_bounds__(QB_THREADS, 1) k_qaoa(QaoaArgs A)
         const int layer = fwd ? r / 2 : P - 1 - r / 2;
         const bool high = fwd ? (r & 1) : !(r & 1);
         for (uint64_t item = blockIdx.x; item < A.n_items; item += gridDim.x) {
-            int lo = 0, hi = A.n_inst;                 // inst[lo].item_off <= item < inst[hi].item_off
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (A.inst[mid].item_off <= item) lo = mid; else hi = mid;
-            }
+            const int lo = (int)A.item_inst[item];
             const QaoaDesc D = A.inst[lo];
             const int n = (int)D.n;
             if (high && n <= M) continue;               // one-tile instance: no high pass
@@ -298,8 +340,8 @@ __global__ void __launch_bounds__(QB_THREADS, 1) k_qaoa(QaoaArgs A)
             const int jb = high ? tm.g : 0;
             const int je = high ? M : min(n, M);
             const bool last_fwd = fwd && layer == P - 1 && (high || n <= M);
-            const double gamma = A.gammas[lo * P + layer], beta = A.betas[lo * P + layer];
-            const T c = static_cast<T>(cos(beta)), s = static_cast<T>(-sin(beta));
+            const double gamma = A.gammas[lo * P + layer];
+            const T c = static_cast<T>(A.mix[2 * (lo * P + layer)]), s = static_cast<T>(A.mix[2 * (lo * P + layer) + 1]);
             const T gam = static_cast<T>(gamma);
             V* gp = psi + D.state_off;
             V* gl = lam + D.state_off;
@@ -341,27 +383,25 @@ __global__ void __launch_bounds__(QB_THREADS, 1) k_qaoa(QaoaArgs A)
             }
             // stages 0..3: mixer on the owned bits, with exchanges between stages
             if (fwd) {
+                // the exchanges alternate between the two buffers (lambda's is free on the
+                // forward sweep), so a buffer is written again only after a barrier that
+                // every read of it precedes
                 stage_rx<T, 0, false>(ps, ls, jb, je, c, s, part_b);
                 exchange<T, 0, 1>(ps, bp, tb0, tb1);
                 stage_rx<T, 1, false>(ps, ls, jb, je, c, s, part_b);
-                __syncthreads();
-                exchange<T, 1, 2>(ps, bp, tb1, tb2);
+                exchange<T, 1, 2>(ps, bl, tb1, tb2);
                 stage_rx<T, 2, false>(ps, ls, jb, je, c, s, part_b);
-                __syncthreads();
                 exchange<T, 2, 3>(ps, bp, tb2, tb3);
                 stage_rx<T, 3, false>(ps, ls, jb, je, c, s, part_b);
             } else {
                 stage_rx<T, 0, true>(ps, ls, jb, je, c, s, part_b);
-                exchange<T, 0, 1>(ps, bp, tb0, tb1);
-                exchange<T, 0, 1>(ls, bl, tb0, tb1);
+                exchange2<T, 0, 1>(ps, ls, bp, bl, tb0, tb1);
                 stage_rx<T, 1, true>(ps, ls, jb, je, c, s, part_b);
                 __syncthreads();
-                exchange<T, 1, 2>(ps, bp, tb1, tb2);
-                exchange<T, 1, 2>(ls, bl, tb1, tb2);
+                exchange2<T, 1, 2>(ps, ls, bp, bl, tb1, tb2);
                 stage_rx<T, 2, true>(ps, ls, jb, je, c, s, part_b);
                 __syncthreads();
-                exchange<T, 2, 3>(ps, bp, tb2, tb3);
-                exchange<T, 2, 3>(ls, bl, tb2, tb3);
+                exchange2<T, 2, 3>(ps, ls, bp, bl, tb2, tb3);
                 stage_rx<T, 3, true>(ps, ls, jb, je, c, s, part_b);
             }
             // stage 3: diagonal work on the final layout, then registers -> HBM
@@ -411,11 +451,11 @@ __global__ void __launch_bounds__(QB_THREADS, 1) k_qaoa(QaoaArgs A)
                 if (threadIdx.x == 0) pt[0] = v;
             }
             if (!fwd) {
-                const double vb = block_sum(part_b, red);
-                if (threadIdx.x == 0) pt[1 + (high ? 2 * P : P) + layer] = 2.0 * vb;
-                if (!high) {
-                    const double vg = block_sum(part_g, red);
-                    if (threadIdx.x == 0) pt[1 + layer] = 2.0 * vg;
+                double vb, vg;
+                block_sum2(part_b, part_g, red, vb, vg);
+                if (threadIdx.x == 0) {
+                    pt[1 + (high ? 2 * P : P) + layer] = 2.0 * vb;
+                    if (!high) pt[1 + layer] = 2.0 * vg;
                 }
             }
             __syncthreads();
@@ -489,7 +529,8 @@ struct svb_qaoa_batch {
     void* lam = nullptr;
     void* cost = nullptr;
     QaoaDesc* d_inst = nullptr;
-    double* d_params = nullptr;      // gammas then betas
+    uint32_t* d_item_inst = nullptr; // instance of each tile of a pass
+    double* d_params = nullptr;      // gammas, betas, then (cos beta, -sin beta) pairs
     double* d_partial = nullptr;
     double* d_out = nullptr;         // energies then gradients
     unsigned* d_bar = nullptr;       // barrier counter, error flag
@@ -513,6 +554,7 @@ void free_batch(svb_qaoa_batch* b)
     cudaFree(b->lam);
     cudaFree(b->cost);
     cudaFree(b->d_inst);
+    cudaFree(b->d_item_inst);
     cudaFree(b->d_params);
     cudaFree(b->d_partial);
     cudaFree(b->d_out);
@@ -527,7 +569,7 @@ template <typename T>
 cudaError_t setup_kernel(svb_qaoa_batch* b)
 {
     using V = typename AmpOf<T>::type;
-    b->smem = 2 * (sizeof(V) << QbCfg<T>::M) + (QB_THREADS / 32) * sizeof(double);
+    b->smem = 2 * (sizeof(V) << QbCfg<T>::M) + 2 * (QB_THREADS / 32) * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(k_qaoa<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0, sms = 0;
@@ -547,8 +589,9 @@ cudaError_t launch_batch(svb_qaoa_batch* b, cudaStream_t s)
     a.lam = b->lam;
     a.cost = b->cost;
     a.inst = b->d_inst;
+    a.item_inst = b->d_item_inst;
     a.gammas = b->d_params;
-    a.betas = b->d_params + (size_t)b->n_inst * b->p;
+    a.mix = b->d_params + (size_t)2 * b->n_inst * b->p;
     a.partial = b->d_partial;
     a.energy = b->d_out;
     a.grad = b->d_out + b->n_inst;
@@ -571,7 +614,7 @@ cudaError_t launch_any(svb_qaoa_batch* b, cudaStream_t s)
 // host pinned params -> device, launch, device results and error flag -> host pinned
 cudaError_t enqueue_run(svb_qaoa_batch* b, cudaStream_t s)
 {
-    const size_t np = (size_t)2 * b->n_inst * b->p;
+    const size_t np = (size_t)4 * b->n_inst * b->p;
     const size_t no = (size_t)b->n_inst * (1 + 2 * b->p);
     cudaError_t e = cudaMemcpyAsync(b->d_params, b->h_params, np * 8, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return e;
@@ -669,16 +712,27 @@ svb_status svb_qaoa_create(int device, int precision, uint32_t n_instances, cons
     if ((e = cudaMalloc(&b->lam, amps * amp_bytes)) != cudaSuccess) return fail("co-state", e);
     if ((e = cudaMalloc(&b->cost, amps * cost_bytes)) != cudaSuccess) return fail("cost table", e);
     if ((e = cudaMalloc(&b->d_inst, desc.size() * sizeof(QaoaDesc))) != cudaSuccess) return fail("alloc", e);
-    if ((e = cudaMalloc(&b->d_params, (size_t)2 * n_instances * p * 8)) != cudaSuccess) return fail("alloc", e);
+    if ((e = cudaMalloc(&b->d_params, (size_t)4 * n_instances * p * 8)) != cudaSuccess) return fail("alloc", e);
     if ((e = cudaMalloc(&b->d_partial, items * nq * 8)) != cudaSuccess) return fail("alloc", e);
     if ((e = cudaMalloc(&b->d_out, (size_t)n_instances * nout * 8)) != cudaSuccess) return fail("alloc", e);
     if ((e = cudaMalloc(&b->d_bar, 2 * sizeof(unsigned))) != cudaSuccess) return fail("alloc", e);
-    if ((e = cudaMallocHost(&b->h_params, (size_t)2 * n_instances * p * 8)) != cudaSuccess) return fail("alloc", e);
+    if ((e = cudaMallocHost(&b->h_params, (size_t)4 * n_instances * p * 8)) != cudaSuccess) return fail("alloc", e);
     if ((e = cudaMallocHost(&b->h_out, (size_t)n_instances * nout * 8)) != cudaSuccess) return fail("alloc", e);
     if ((e = cudaMallocHost(&b->h_err, sizeof(unsigned))) != cudaSuccess) return fail("alloc", e);
-    std::memset(b->h_params, 0, (size_t)2 * n_instances * p * 8);
+    std::memset(b->h_params, 0, (size_t)4 * n_instances * p * 8);
     if ((e = cudaMemcpy(b->d_inst, desc.data(), desc.size() * sizeof(QaoaDesc), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail("upload", e);
+    {
+        std::vector<uint32_t> item_inst(std::max<uint64_t>(items, 1), 0);
+        for (uint32_t i = 0; i < n_instances; i++) {
+            const uint64_t end = i + 1 < n_instances ? desc[i + 1].item_off : items;
+            for (uint64_t t = desc[i].item_off; t < end; t++) item_inst[t] = i;
+        }
+        if ((e = cudaMalloc(&b->d_item_inst, item_inst.size() * 4)) != cudaSuccess) return fail("alloc", e);
+        if ((e = cudaMemcpy(b->d_item_inst, item_inst.data(), item_inst.size() * 4, cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return fail("upload", e);
+    }
     // the high-pass entries of one-tile instances are never written: zero them once
     if ((e = cudaMemset(b->d_partial, 0, items * nq * 8)) != cudaSuccess) return fail("memset", e);
     if ((e = cudaMalloc(&d_eoff, eoff.size() * 4)) != cudaSuccess ||
@@ -733,6 +787,10 @@ svb_status svb_qaoa_run(svb_qaoa_batch* b, const double* gammas, const double* b
     const size_t np = (size_t)b->n_inst * b->p;
     std::memcpy(b->h_params, gammas, np * 8);
     std::memcpy(b->h_params + np, betas, np * 8);
+    for (size_t i = 0; i < np; i++) {             // the mixer's RX(2 beta) coefficients
+        b->h_params[2 * np + 2 * i] = std::cos(betas[i]);
+        b->h_params[2 * np + 2 * i + 1] = -std::sin(betas[i]);
+    }
     *b->h_err = 0;
     e = b->graphed ? cudaGraphLaunch(b->graph, b->stream) : enqueue_run(b, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
