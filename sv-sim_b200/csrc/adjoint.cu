@@ -26,9 +26,6 @@ namespace {
 constexpr int ADJ_BLOCKS = 296;   // 2 x 148 SMs
 constexpr int ADJ_THREADS = 256;
 
-struct DMats {
-    double d[3][8];   // up to three derivative matrices, C1 layout
-};
 
 __device__ __forceinline__ double block_sum(double v, double* red)
 {
@@ -43,61 +40,157 @@ __device__ __forceinline__ double block_sum(double v, double* red)
     return s;
 }
 
-// One reverse step of a single-qubit elementary op (inverse applied as F_C1/F_DIAG).
-__global__ void __launch_bounds__(ADJ_THREADS)
-k_adj_step(double2* __restrict__ psi, double2* __restrict__ lam, uint64_t half, int q, int form,
-           Coef<double> inv, int nd, DMats dm, double* __restrict__ partial)
-{
-    __shared__ double red[ADJ_THREADS / 32];
-    double acc[3] = {0.0, 0.0, 0.0};
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t qd = 1ull << q;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < half; i += stride) {
-        const uint64_t p0 = insert_zero(i, q), p1 = p0 | qd;
-        double2 s0 = psi[p0], s1 = psi[p1];
-        double2 l0 = lam[p0], l1 = lam[p1];
-        if (form == F_DIAG) {
-            diag_zero<double>(F_DIAG, inv, s0);
-            diag_one<double>(F_DIAG, inv, s1);
-        } else {
-            dense_pair<double>(F_C1, inv, s0, s1);
-        }
-        for (int d = 0; d < nd; d++) {
-            const double* m = dm.d[d];
-            const double u0r = m[0] * s0.x - m[1] * s0.y + m[2] * s1.x - m[3] * s1.y;
-            const double u0i = m[0] * s0.y + m[1] * s0.x + m[2] * s1.y + m[3] * s1.x;
-            const double u1r = m[4] * s0.x - m[5] * s0.y + m[6] * s1.x - m[7] * s1.y;
-            const double u1i = m[4] * s0.y + m[5] * s0.x + m[6] * s1.y + m[7] * s1.x;
-            acc[d] += l0.x * u0r + l0.y * u0i + l1.x * u1r + l1.y * u1i;
-        }
-        if (form == F_DIAG) {
-            diag_zero<double>(F_DIAG, inv, l0);
-            diag_one<double>(F_DIAG, inv, l1);
-        } else {
-            dense_pair<double>(F_C1, inv, l0, l1);
-        }
-        psi[p0] = s0; psi[p1] = s1;
-        lam[p0] = l0; lam[p1] = l1;
-    }
-    for (int d = 0; d < nd; d++) {
-        const double s = block_sum(acc[d], red);
-        if (threadIdx.x == 0) partial[(size_t)d * ADJ_BLOCKS + blockIdx.x] = s;
-    }
-}
+// ---- the reverse sweep, tiled -------------------------------------------------------
+// The inverse ops in reverse order are cut into passes (select_passes) of AT_M local
+// qubits.  A CTA loads a tile of psi and of lambda into shared memory, applies the pass's
+// ops in order (for each: psi <- U^dagger psi, the derivative sums Re <lambda| dU |psi>,
+// lambda <- U^dagger lambda) and writes the tile back; a differentiated op leaves one
+// block-reduced sum per tile and slot in `partial` (row = slot, column = tile).
+constexpr int AT_M = 10;                  // 1,024 amplitudes of psi and of lambda: 32 KiB
+constexpr int AT_THREADS = 256;
 
-__global__ void __launch_bounds__(ADJ_THREADS)
-k_adj_cx(double2* __restrict__ psi, double2* __restrict__ lam, uint64_t quarter, int c, int t)
+enum { AT_C1 = 0, AT_DIAG = 1, AT_CX = 2 };
+
+struct AdjTileOp {
+    uint8_t kind;      // AT_C1 (target local), AT_DIAG, AT_CX (target local)
+    uint8_t p;         // local position of the target
+    uint8_t c;         // AT_CX: local position of the control
+    uint8_t flags;     // bit 0: the DIAG qubit is a tile bit; bit 1: the CX control is
+    uint8_t nd;        // derivative slots (AT_C1 only)
+    uint8_t tile_bit;  // tile-index bit of a tile-bit qubit
+    uint8_t pad[2];
+    int32_t slot;      // first derivative slot
+    int32_t pad2;
+    double m[8];       // the inverse op: C1 2x2, or d0, d1 for DIAG
+    double dm[3][8];   // derivative matrices, C1 layout
+};
+static_assert(sizeof(AdjTileOp) % 16 == 0, "AdjTileOp layout");
+
+struct AdjTilePass {
+    uint8_t nonlocal_q[64];
+    uint64_t g_lo[64];         // local index bits 0-5 -> global offset
+    uint64_t g_hi[32];         // local index bits 6-10 -> global offset
+    int32_t n_nonlocal, op_begin, op_end, pad;
+};
+static_assert(sizeof(AdjTilePass) % 16 == 0, "AdjTilePass layout");
+
+__global__ void __launch_bounds__(AT_THREADS, 3)
+k_adj_tiles(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTilePass* __restrict__ passes,
+            int pass_index, const AdjTileOp* __restrict__ ops, int M, uint64_t tiles,
+            double* __restrict__ partial)
 {
-    const int lo = c < t ? c : t, hi = c < t ? t : c;
-    const uint64_t cd = 1ull << c, td = 1ull << t;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < quarter; i += stride) {
-        const uint64_t b = insert_zero(insert_zero(i, lo), hi);
-        const uint64_t p0 = b | cd, p1 = b | cd | td;
-        const double2 a0 = psi[p0], a1 = psi[p1];
-        psi[p0] = a1; psi[p1] = a0;
-        const double2 b0 = lam[p0], b1 = lam[p1];
-        lam[p0] = b1; lam[p1] = b0;
+    extern __shared__ __align__(16) double2 at_sm[];
+    __shared__ AdjTilePass P;
+    __shared__ double red[AT_THREADS / 32];
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(passes + pass_index);
+        uint4* dst = reinterpret_cast<uint4*>(&P);
+        for (int w = threadIdx.x; w < (int)(sizeof(AdjTilePass) / 16); w += AT_THREADS) dst[w] = src[w];
+        __syncthreads();
+    }
+    const uint32_t T = 1u << M;
+    double2* sp = at_sm;
+    double2* sl = at_sm + T;
+    for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        uint64_t base = 0;
+        for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
+        for (uint32_t l = threadIdx.x; l < T; l += AT_THREADS) {
+            const uint64_t g = base + P.g_lo[l & 63u] + P.g_hi[l >> 6];
+            sp[l] = psi[g];
+            sl[l] = lam[g];
+        }
+        __syncthreads();
+        for (int o = P.op_begin; o < P.op_end; o++) {
+            const AdjTileOp& op = ops[o];
+            const uint4 hdr = __ldg(reinterpret_cast<const uint4*>(&op));
+            const int kind = hdr.x & 0xFFu, p = (hdr.x >> 8) & 0xFFu, flags = hdr.x >> 24;
+            const int nd = hdr.y & 0xFFu, tbit = (hdr.y >> 8) & 0xFFu, slot = (int)hdr.z;
+            Coef<double> inv;
+            {
+                const double2* m2 = reinterpret_cast<const double2*>(op.m);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const double2 v = __ldg(m2 + j);
+                    inv.m[2 * j] = v.x;
+                    inv.m[2 * j + 1] = v.y;
+                }
+            }
+            if (kind == AT_C1) {
+                double acc[3] = {0.0, 0.0, 0.0};
+                for (uint32_t i = threadIdx.x; i < T / 2; i += AT_THREADS) {
+                    const uint32_t p0 = (uint32_t)insert_zero(i, p), p1 = p0 | (1u << p);
+                    double2 s0 = sp[p0], s1 = sp[p1];
+                    double2 l0 = sl[p0], l1 = sl[p1];
+                    dense_pair<double>(F_C1, inv, s0, s1);
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {
+                        if (d >= nd) break;
+                        double m[8];
+                        const double2* m2 = reinterpret_cast<const double2*>(op.dm[d]);
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            const double2 v = __ldg(m2 + j);
+                            m[2 * j] = v.x;
+                            m[2 * j + 1] = v.y;
+                        }
+                        const double u0r = m[0] * s0.x - m[1] * s0.y + m[2] * s1.x - m[3] * s1.y;
+                        const double u0i = m[0] * s0.y + m[1] * s0.x + m[2] * s1.y + m[3] * s1.x;
+                        const double u1r = m[4] * s0.x - m[5] * s0.y + m[6] * s1.x - m[7] * s1.y;
+                        const double u1i = m[4] * s0.y + m[5] * s0.x + m[6] * s1.y + m[7] * s1.x;
+                        acc[d] += l0.x * u0r + l0.y * u0i + l1.x * u1r + l1.y * u1i;
+                    }
+                    dense_pair<double>(F_C1, inv, l0, l1);
+                    sp[p0] = s0; sp[p1] = s1;
+                    sl[p0] = l0; sl[p1] = l1;
+                }
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    if (d >= nd) break;
+                    const double v = block_sum(acc[d], red);
+                    if (threadIdx.x == 0) partial[(uint64_t)(slot + d) * tiles + tile] = v;
+                }
+            } else if (kind == AT_DIAG) {
+                const bool tile_bit = flags & 1;
+                const bool one_tile = tile_bit && ((tile >> tbit) & 1ull);
+                for (uint32_t l = threadIdx.x; l < T; l += AT_THREADS) {
+                    const bool one = tile_bit ? one_tile : ((l >> p) & 1u);
+                    double2 a = sp[l], b = sl[l];
+                    if (one) { diag_one<double>(F_DIAG, inv, a); diag_one<double>(F_DIAG, inv, b); }
+                    else { diag_zero<double>(F_DIAG, inv, a); diag_zero<double>(F_DIAG, inv, b); }
+                    sp[l] = a;
+                    sl[l] = b;
+                }
+            } else {
+                const uint32_t pd = 1u << p;
+                if (flags & 2) {
+                    if ((tile >> tbit) & 1ull) {
+                        for (uint32_t i = threadIdx.x; i < T / 2; i += AT_THREADS) {
+                            const uint32_t p0 = (uint32_t)insert_zero(i, p), p1 = p0 | pd;
+                            const double2 a0 = sp[p0], a1 = sp[p1], b0 = sl[p0], b1 = sl[p1];
+                            sp[p0] = a1; sp[p1] = a0;
+                            sl[p0] = b1; sl[p1] = b0;
+                        }
+                    }
+                } else {
+                    const int c = (hdr.x >> 16) & 0xFFu;
+                    const int lo = c < p ? c : p, hi = c < p ? p : c;
+                    for (uint32_t i = threadIdx.x; i < T / 4; i += AT_THREADS) {
+                        const uint32_t b = (uint32_t)insert_zero(insert_zero(i, lo), hi) | (1u << c);
+                        const uint32_t p0 = b, p1 = b | pd;
+                        const double2 a0 = sp[p0], a1 = sp[p1], b0 = sl[p0], b1 = sl[p1];
+                        sp[p0] = a1; sp[p1] = a0;
+                        sl[p0] = b1; sl[p1] = b0;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        for (uint32_t l = threadIdx.x; l < T; l += AT_THREADS) {
+            const uint64_t g = base + P.g_lo[l & 63u] + P.g_hi[l >> 6];
+            psi[g] = sp[l];
+            lam[g] = sl[l];
+        }
+        __syncthreads();
     }
 }
 
@@ -146,16 +239,15 @@ k_inner_re(const double2* __restrict__ a, const double2* __restrict__ b, uint64_
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
-// results[r] = sum of partial[r * ADJ_BLOCKS + i], i < nblocks (the blocks the producing
-// kernels ran with); one warp per result, fixed order
-__global__ void k_reduce_rows(const double* __restrict__ partial, int nblocks, int rows,
+// results[r] = sum of partial[r * stride + i], i < nblocks; one warp per result, fixed order
+__global__ void k_reduce_rows(const double* __restrict__ partial, int nblocks, uint64_t stride, int rows,
                               double* __restrict__ results)
 {
     const int lane = threadIdx.x & 31;
     const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (row >= rows) return;
     double s = 0.0;
-    for (int i = lane; i < nblocks; i += 32) s += partial[(size_t)row * ADJ_BLOCKS + i];
+    for (int i = lane; i < nblocks; i += 32) s += partial[(size_t)row * stride + i];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) results[row] = s;
@@ -294,12 +386,12 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
                           std::to_string(bindings[i].idx[f]) + " >= n_params");
                 return SVB_ERR_INVALID;
             }
-    // validates the gates, builds the forward plan and replaces the circuit
-    svb_status rc = svb_set_circuit(s, gates, n_gates);
+    // validates and lowers the gates; the handle's own circuit and plan stay as they are
+    std::vector<EOp> eops;
+    svb_status rc = validate_and_lower(s, gates, n_gates, eops, nullptr);
     if (rc != SVB_OK) return rc;
     const int n = (int)s->n;
     const uint64_t dim = 1ull << n;
-    const std::vector<EOp> eops = s->eops;
     const size_t K = eops.size();
 
     // derivative slots
@@ -343,8 +435,11 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
         return e == cudaErrorMemoryAllocation ? SVB_ERR_OOM : SVB_ERR_CUDA;
     };
     const size_t nslots = std::max<size_t>(slots.size(), 1);
+    const int TM = std::min(n, AT_M);                 // local qubits of a reverse-sweep tile
+    const uint64_t tiles = 1ull << (n - TM);
+    const size_t eoff = slots.size() * tiles;         // the energy's partials follow the slots'
     if ((err = grow(A.lam, sbytes)) != cudaSuccess) return fail(err, "cudaMalloc(lambda)");
-    if ((err = grow(A.partial, (nslots + 1) * ADJ_BLOCKS * sizeof(double))) != cudaSuccess)
+    if ((err = grow(A.partial, (nslots * tiles + ADJ_BLOCKS) * sizeof(double))) != cudaSuccess)
         return fail(err, "cudaMalloc(partials)");
     if ((err = grow(A.results, (nslots + 1) * sizeof(double))) != cudaSuccess)
         return fail(err, "cudaMalloc(results)");
@@ -401,41 +496,129 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
             static_cast<const double2*>(s->state), lam, dim, dterms, (int)n_terms);
     else
         err = cudaMemset(lam, 0, sbytes);
-    k_inner_re<<<ADJ_BLOCKS, 256>>>(static_cast<const double2*>(s->state), lam, dim,
-                                     partial + slots.size() * ADJ_BLOCKS);
-    k_reduce_rows<<<1, 32>>>(partial + slots.size() * ADJ_BLOCKS, ADJ_BLOCKS, 1, results + slots.size());
+    k_inner_re<<<ADJ_BLOCKS, 256>>>(static_cast<const double2*>(s->state), lam, dim, partial + eoff);
+    k_reduce_rows<<<1, 32>>>(partial + eoff, ADJ_BLOCKS, ADJ_BLOCKS, 1, results + slots.size());
     if ((err = cudaGetLastError()) != cudaSuccess) return fail(err, "energy");
 
-    // reverse sweep
-    double2* psi = static_cast<double2*>(s->state);
-    int ck = (int)ckpts.size() - 1;
-    const unsigned gp = adj_grid(dim / 2);
-    for (size_t kk = K; kk-- > 0;) {
-        const EOp& e = eops[kk];
-        EOp inv;
-        inverse_op(e, inv);
-        if (inv.form == F_CX) {
-            k_adj_cx<<<adj_grid(dim / 4), ADJ_THREADS>>>(psi, lam, dim / 4, (int)e.c, (int)e.q);
-        } else {
-            DMats dm;
-            std::memset(&dm, 0, sizeof(dm));
-            const int nd = n_slot[kk];
-            for (int d = 0; d < nd; d++) deriv_matrix(e, slots[first_slot[kk] + d].i, dm.d[d]);
-            Coef<double> ci;
-            for (int j = 0; j < 8; j++) ci.m[j] = inv.m[j];
-            double* part = nd ? partial + (size_t)first_slot[kk] * ADJ_BLOCKS : partial;
-            k_adj_step<<<gp, ADJ_THREADS>>>(psi, lam, dim / 2, (int)e.q, inv.form, ci, nd, dm, part);
+    // reverse sweep, tiled: the inverse ops in reverse order, cut into passes of TM local
+    // qubits; a pass never spans a checkpoint, after which psi is reloaded
+    std::vector<AdjTilePass> tpasses;
+    std::vector<AdjTileOp> tops;
+    struct Seg { size_t pass_end; int ck; };          // reload checkpoint ck after the passes
+    std::vector<Seg> segs;
+    {
+        const int G = std::min(4, TM);
+        size_t kk_hi = K;
+        for (int ck = (int)ckpts.size() - 1;; ck--) {
+            const size_t kk_lo = ck >= 0 ? ckpt_at[ck] : 0;
+            std::vector<EOp> rev;
+            std::vector<size_t> orig;
+            for (size_t kk = kk_hi; kk-- > kk_lo;) {
+                EOp inv;
+                inverse_op(eops[kk], inv);
+                if (n_slot[kk] > 0 && inv.form == F_DIAG) {
+                    // a differentiated op needs its pairs local: as a general 2x2
+                    const double d0r = inv.m[0], d0i = inv.m[1], d1r = inv.m[2], d1i = inv.m[3];
+                    inv.form = F_C1;
+                    const double c1[8] = {d0r, d0i, 0, 0, 0, 0, d1r, d1i};
+                    std::memcpy(inv.m, c1, sizeof(c1));
+                }
+                rev.push_back(inv);
+                orig.push_back(kk);
+            }
+            select_passes(rev, n, TM, G, [&](uint64_t L, const std::vector<int>& idx) {
+                AdjTilePass P;
+                std::memset(&P, 0, sizeof(P));
+                int pos[64], tbit[64];
+                uint8_t local_q[AT_M];
+                int nl = 0, nn = 0;
+                for (int q = 0; q < 64; q++) pos[q] = tbit[q] = -1;
+                for (int q = 0; q < n; q++) {
+                    if ((L >> q) & 1ull) { pos[q] = nl; local_q[nl++] = (uint8_t)q; }
+                    else { tbit[q] = nn; P.nonlocal_q[nn++] = (uint8_t)q; }
+                }
+                P.n_nonlocal = nn;
+                for (int j = 0; j < 64; j++)
+                    for (int b2 = 0; b2 < 6 && b2 < TM; b2++)
+                        if ((j >> b2) & 1) P.g_lo[j] |= 1ull << local_q[b2];
+                for (int j = 0; j < 32; j++)
+                    for (int b2 = 0; b2 < 5 && 6 + b2 < TM; b2++)
+                        if ((j >> b2) & 1) P.g_hi[j] |= 1ull << local_q[6 + b2];
+                P.op_begin = (int32_t)tops.size();
+                for (int i : idx) {
+                    const EOp& e = rev[i];
+                    const size_t kk = orig[i];
+                    AdjTileOp t;
+                    std::memset(&t, 0, sizeof(t));
+                    if (e.form == F_CX) {
+                        t.kind = AT_CX;
+                        t.p = (uint8_t)pos[e.q];
+                        if (pos[e.c] >= 0) t.c = (uint8_t)pos[e.c];
+                        else { t.flags |= 2; t.tile_bit = (uint8_t)tbit[e.c]; }
+                    } else if (e.form == F_DIAG) {
+                        t.kind = AT_DIAG;
+                        std::memcpy(t.m, e.m, sizeof(t.m));
+                        if (pos[e.q] >= 0) t.p = (uint8_t)pos[e.q];
+                        else { t.flags |= 1; t.tile_bit = (uint8_t)tbit[e.q]; }
+                    } else {
+                        t.kind = AT_C1;
+                        t.p = (uint8_t)pos[e.q];
+                        std::memcpy(t.m, e.m, sizeof(t.m));
+                        t.nd = (uint8_t)n_slot[kk];
+                        t.slot = first_slot[kk];
+                        for (int d = 0; d < n_slot[kk]; d++) deriv_matrix(eops[kk], slots[first_slot[kk] + d].i, t.dm[d]);
+                    }
+                    tops.push_back(t);
+                }
+                P.op_end = (int32_t)tops.size();
+                tpasses.push_back(P);
+                return std::vector<int>{};
+            });
+            segs.push_back({tpasses.size(), ck});
+            kk_hi = kk_lo;
+            if (ck < 0) break;
         }
-        if ((err = cudaGetLastError()) != cudaSuccess) return fail(err, "reverse step");
-        // psi is now the state before op kk; reload the stored copy if there is one
-        if (ck >= 0 && ckpt_at[ck] == kk) {
-            if ((err = cudaMemcpyAsync(psi, ckpts[ck], sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
+    }
+    if ((err = grow(A.rev_passes, std::max<size_t>(1, tpasses.size()) * sizeof(AdjTilePass))) != cudaSuccess)
+        return fail(err, "cudaMalloc(reverse plan)");
+    if ((err = grow(A.rev_ops, std::max<size_t>(1, tops.size()) * sizeof(AdjTileOp))) != cudaSuccess)
+        return fail(err, "cudaMalloc(reverse plan)");
+    if (!tpasses.empty() && (err = cudaMemcpyAsync(A.rev_passes.p, tpasses.data(), tpasses.size() * sizeof(AdjTilePass),
+                                                   cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(err, "reverse plan upload");
+    if (!tops.empty() && (err = cudaMemcpyAsync(A.rev_ops.p, tops.data(), tops.size() * sizeof(AdjTileOp),
+                                                cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(err, "reverse plan upload");
+    double2* psi = static_cast<double2*>(s->state);
+    {
+        static int ctas_per_sm = 0, sms = 0;
+        const size_t smem = 2 * sizeof(double2) << AT_M;
+        if (ctas_per_sm == 0) {
+            if ((err = cudaFuncSetAttribute(k_adj_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+                    cudaSuccess ||
+                (err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, k_adj_tiles, AT_THREADS, smem)) !=
+                    cudaSuccess ||
+                (err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device)) != cudaSuccess)
+                return fail(err, "reverse kernel setup");
+            ctas_per_sm = std::max(ctas_per_sm, 1);
+        }
+        const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)ctas_per_sm * sms);
+        const size_t dyn = 2 * sizeof(double2) << TM;
+        size_t pi = 0;
+        for (const Seg& sg : segs) {
+            for (; pi < sg.pass_end; pi++)
+                k_adj_tiles<<<grid, AT_THREADS, dyn>>>(psi, lam, static_cast<const AdjTilePass*>(A.rev_passes.p),
+                                                       (int)pi, static_cast<const AdjTileOp*>(A.rev_ops.p), TM,
+                                                       tiles, partial);
+            if ((err = cudaGetLastError()) != cudaSuccess) return fail(err, "reverse pass");
+            // psi is now the state before op ckpt_at[ck]: reload the stored copy
+            if (sg.ck >= 0 &&
+                (err = cudaMemcpyAsync(psi, ckpts[sg.ck], sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
                 return fail(err, "checkpoint reload");
-            ck--;
         }
     }
     if (!slots.empty())
-        k_reduce_rows<<<(unsigned)((slots.size() * 32 + 255) / 256), 256>>>(partial, (int)gp,
+        k_reduce_rows<<<(unsigned)((slots.size() * 32 + 255) / 256), 256>>>(partial, (int)tiles, tiles,
                                                                           (int)slots.size(), results);
     std::vector<double> host(slots.size() + 1);
     if ((err = cudaMemcpy(host.data(), results, host.size() * sizeof(double), cudaMemcpyDeviceToHost)) !=

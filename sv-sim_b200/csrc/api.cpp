@@ -228,6 +228,8 @@ void free_adjoint_scratch(AdjScratch& a)
     release(a.plan_passes);
     release(a.plan_stages);
     release(a.plan_ops);
+    release(a.rev_passes);
+    release(a.rev_ops);
     for (GrowBuf& b : a.ckpts) release(b);
     a.ckpts.clear();
 }
@@ -269,6 +271,43 @@ svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cuda
 }  // namespace svb
 
 using namespace svb;
+
+namespace svb {
+
+// Checks every gate record against the handle (op known, qubits < n, no repeats; the
+// reference asserts qb0..qb4 < n_qubits for every gate, :259-264) and lowers the
+// circuit to elementary ops; `sweeps` gets the reference's per-gate sweep count.
+svb_status validate_and_lower(Sim* s, const svb_gate* gates, size_t n_gates, std::vector<EOp>& eops,
+                              double* sweeps)
+{
+    if (n_gates > 0 && !gates) return invalid("svb_set_circuit: gates is NULL");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    for (size_t i = 0; i < n_gates; i++) {
+        const svb_gate& g = gates[i];
+        const int k = n_qubit_slots(g.op);
+        if (k == 0) return invalid("gate " + std::to_string(i) + ": unknown op " + std::to_string(g.op));
+        for (int j = 0; j < 5; j++)
+            if (g.qb[j] >= s->n)
+                return invalid("gate " + std::to_string(i) + ": qubit index " +
+                               std::to_string(g.qb[j]) + " >= n_qubits");
+        for (int a = 0; a < k; a++)
+            for (int b = a + 1; b < k; b++)
+                if (g.qb[a] == g.qb[b])
+                    return invalid("gate " + std::to_string(i) + ": repeated qubit " +
+                                   std::to_string(g.qb[a]));
+    }
+    eops.clear();
+    eops.reserve(n_gates * 2);
+    double sw = 0;
+    for (size_t i = 0; i < n_gates; i++) {
+        lower_gate(gates[i], (int32_t)i, eops);
+        sw += reference_sweeps(gates[i].op);
+    }
+    if (sweeps) *sweeps = sw;
+    return SVB_OK;
+}
+
+}  // namespace svb
 
 extern "C" {
 
@@ -364,31 +403,10 @@ svb_status svb_set_engine(svb_sim* s, int engine, int tile_bits, int fusion_widt
 svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
 {
     if (!s) return invalid("svb_set_circuit: NULL handle");
-    if (n_gates > 0 && !gates) return invalid("svb_set_circuit: gates is NULL");
-    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
-    // validate everything before touching the current plan
-    for (size_t i = 0; i < n_gates; i++) {
-        const svb_gate& g = gates[i];
-        const int k = n_qubit_slots(g.op);
-        if (k == 0) return invalid("gate " + std::to_string(i) + ": unknown op " + std::to_string(g.op));
-        // the reference asserts qb0..qb4 < n_qubits for every gate (:259-264)
-        for (int j = 0; j < 5; j++)
-            if (g.qb[j] >= s->n)
-                return invalid("gate " + std::to_string(i) + ": qubit index " +
-                               std::to_string(g.qb[j]) + " >= n_qubits");
-        for (int a = 0; a < k; a++)
-            for (int b = a + 1; b < k; b++)
-                if (g.qb[a] == g.qb[b])
-                    return invalid("gate " + std::to_string(i) + ": repeated qubit " +
-                                   std::to_string(g.qb[a]));
-    }
     std::vector<EOp> eops;
-    eops.reserve(n_gates * 2);
     double sweeps = 0;
-    for (size_t i = 0; i < n_gates; i++) {
-        lower_gate(gates[i], (int32_t)i, eops);
-        sweeps += reference_sweeps(gates[i].op);
-    }
+    const svb_status st = validate_and_lower(s, gates, n_gates, eops, &sweeps);
+    if (st != SVB_OK) return st;
     s->mats.clear();
     return set_circuit_lowered(s, eops, gates, n_gates, sweeps);
 }

@@ -366,6 +366,7 @@ void release(GrowBuf& b);
 struct AdjScratch {
     GrowBuf lam, partial, results, terms, final_state;
     GrowBuf plan_passes, plan_stages, plan_ops;     // forward segments' staged plans
+    GrowBuf rev_passes, rev_ops;                    // the tiled reverse sweep's plan
     std::vector<GrowBuf> ckpts;
 };
 
@@ -374,6 +375,11 @@ struct AdjScratch {
 svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st,
                            AdjScratch& cache);
 void free_adjoint_scratch(AdjScratch& a);
+struct Sim;
+// Validates gate records against the handle and lowers them to elementary ops (the
+// first half of svb_set_circuit, without planning).
+svb_status validate_and_lower(Sim* s, const svb_gate* gates, size_t n_gates, std::vector<EOp>& eops,
+                              double* sweeps);
 
 // ---------------------------------------------------------------------------------
 // The handle
