@@ -238,7 +238,8 @@ svb_status svb_dm_probabilities(svb_sim* sim, double* out);
  * grad[binding.idx] += 2 Re <lambda| dU/dp |psi_prev> * binding.coef in FP64.
  * `gates` carry the angle values at the current parameters; `bindings` (one per gate)
  * say which angles depend on which of the n_params parameters.  Writes energy (may
- * be NULL) and grad[n_params].  The handle's state is left holding psi(p). */
+ * be NULL) and grad[n_params].  The handle's state is left holding psi(p); its circuit
+ * and plan (svb_set_circuit) are not changed. */
 svb_status svb_adjoint(svb_sim* sim, const svb_gate* gates, const svb_param_binding* bindings,
                        size_t n_gates, uint32_t n_params, const svb_pauli_term* terms,
                        size_t n_terms, double* energy, double* grad);

@@ -10,6 +10,9 @@
 // Only psi and lambda are held; to bound the drift of the reverse-propagated psi the
 // forward pass stores checkpoints, and psi is reloaded from them on the way back.
 // Every reduction is FP64 with a fixed order (per-block partials, then one pass).
+// The forward pass runs on the staged engine; the reverse sweep is tiled: its inverse ops
+// are cut into passes of local qubits, and each tile of psi and lambda goes through a
+// pass's ops in shared memory, leaving one derivative sum per tile and parameter slot.
 #include <cmath>
 #include <cstring>
 #include <algorithm>
