@@ -43,8 +43,8 @@ typedef enum svb_precision {
 } svb_precision;
 
 typedef enum svb_engine {
-    SVB_ENGINE_AUTO = 0,      /* FP64 n >= 12 without SRN: pairs; else staged for n >= 10
-                                 (FP32: 11), per-gate below */
+    SVB_ENGINE_AUTO = 0,      /* n >= 12 without SRN: pairs (FP64) or fused (FP32); else
+                                 staged for n >= 10 (FP32: 11), per-gate below */
     SVB_ENGINE_PER_GATE = 1,  /* one HBM sweep per elementary gate, as the reference */
     SVB_ENGINE_STAGED = 2,    /* many gates per HBM sweep through a shared-memory tile */
     SVB_ENGINE_FUSED = 3,     /* gates fused into dense k-qubit blocks (FP32 only) */

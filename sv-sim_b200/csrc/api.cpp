@@ -440,9 +440,11 @@ svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* g
         }
     }
     if (engine == SVB_ENGINE_AUTO) {
-        // FP64 circuits of >= 12 qubits go to the pair engine (FP64 tensor cores) unless they
-        // hold SRN, which has no matrix; otherwise the staged engine, per-gate below its tile
-        if (s->precision == SVB_FP64 && n >= PR_TILE_BITS && fusable(s->eops)) engine = SVB_ENGINE_PAIRS;
+        // Circuits of >= 12 qubits without SRN (which has no matrix) go to the tensor cores:
+        // FP64 to the pair engine, FP32 to the fused engine (2x the staged engine at n = 24
+        // and 30); otherwise the staged engine, per-gate below its tile
+        if (n >= PR_TILE_BITS && fusable(s->eops))
+            engine = s->precision == SVB_FP64 ? SVB_ENGINE_PAIRS : SVB_ENGINE_FUSED;
         else engine = (staged_supported(s->precision, M) && n >= M) ? SVB_ENGINE_STAGED : SVB_ENGINE_PER_GATE;
     }
     if (engine == SVB_ENGINE_FUSED) {

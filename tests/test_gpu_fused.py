@@ -93,3 +93,21 @@ def test_fused_run_keeps_unit_norm_and_small_amplitude_error():
     f, d = h64.compare(h32)
     amp = 2.0 ** (-n / 2)
     assert 1 - f <= 1e-9 and d <= 2e-4 * amp, (1 - f, d)
+
+
+def test_auto_engine_runs_fp32_circuits_on_the_fused_engine(oracle):
+    """AUTO sends FP32 circuits of >= 12 qubits to the fused engine, and those with SRN
+    (not complex-linear) to the staged engine; both match the oracle."""
+    from svsim_b200 import _native as nat
+    n = 14
+    g = circuits.random_matching_circuit(n, 6, seed=21)
+    h = nat.Handle(n, 0, nat.SVB_FP32)
+    h.set_circuit(g)
+    assert h.plan_info().engine == nat.ENGINE_FUSED
+    h.run()
+    re, im = h.get_state()
+    ore, oim = oracle.run(n, g)
+    assert 1 - fidelity(re + 1j * im, ore + 1j * oim) <= 1e-6
+    g2 = G.to_array(G.from_array(g) + [G.SRN(3)])
+    h.set_circuit(g2)
+    assert h.plan_info().engine == nat.ENGINE_STAGED
