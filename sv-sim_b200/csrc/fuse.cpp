@@ -5,10 +5,12 @@
 // every qubit an op touches must be local to the pass.  Inside a pass the ops are
 // grouped into blocks acting on at most k qubits; each block is multiplied out on the
 // host in FP64 into one 2^k x 2^k complex matrix, written as the real 2^(k+1) square
-// [[Re,-Im],[Im,Re]] interleaved by (index, re/im), split into a TF32 "hi" part and an
-// FP32 "lo" remainder, and laid out in the tensor core's canonical K-major shared-memory
-// format.  The kernel (kernels_fused.cu) applies a pass's blocks to a tile in shared
-// memory with tcgen05 MMAs: D = X_hi G_hi^T + X_hi G_lo^T + X_lo G_hi^T.
+// [[Re,-Im],[Im,Re]] interleaved by (index, re/im), split into TF32 G_hi and G_lo (both
+// rounded to nearest from the FP64 value) and stored as one 2N-row operand (G_hi rows,
+// then G_lo rows) in the tensor core's canonical K-major shared-memory format.  The plan
+// also fixes, per pass and block, the bit orders and the XOR-combined tables through which
+// the kernel (kernels_fused.cu) moves a tile between blocks, chosen so that its
+// shared-memory transposes are free of bank conflicts.
 #include <algorithm>
 #include <cmath>
 #include <complex>
