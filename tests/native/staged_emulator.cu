@@ -429,6 +429,12 @@ extern "C" int emu_pairs_stats(uint32_t n, const svb_gate* gates, size_t n_gates
     stats[1] = plan.n_blocks;
     stats[2] = plan.n_swaps;
     stats[3] = plan.n_relayouts;
+    // passes whose gate fragments stay in global memory (too many for shared memory), and
+    // the largest per-pass copy into shared memory
+    uint64_t unstaged = 0;
+    for (const PairPass& P : plan.passes) unstaged += P.stage_gates ? 0 : 1;
+    stats[4] = unstaged;
+    stats[5] = plan.stage_bytes;
     return 0;
 }
 

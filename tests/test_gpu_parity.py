@@ -351,6 +351,17 @@ def test_pair_engine_random_matching_vs_oracle(oracle, n):
     assert_close(re, im, ore, oim)
 
 
+def test_pair_engine_pass_with_gates_beyond_shared_memory(oracle):
+    """n = 12, depth 40: one pass holds more gate fragments than fit beside the tile in
+    shared memory (tests/test_plan.py checks that the plan says so), so the kernel reads
+    that pass's gates from global memory."""
+    nat = native()
+    g = circuits.random_matching_circuit(12, 40, seed=1)
+    ore, oim = oracle.run(12, g)
+    _, re, im = run_gpu(12, g, nat.ENGINE_PAIRS)
+    assert_close(re, im, ore, oim)
+
+
 @pytest.mark.parametrize("n", [12, 15])
 def test_pair_engine_every_op_but_srn(oracle, n):
     nat = native()

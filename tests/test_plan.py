@@ -181,3 +181,24 @@ def test_pair_plan_rejects_srn_and_small_states(emu):
     g = G.to_array([G.H(0), G.SRN(1)])
     assert run_pairs_emu(emu, 12, g)[0] == -6
     assert run_pairs_emu(emu, 11, G.to_array([G.H(0)]))[0] == -6
+
+
+def test_pair_plan_shared_memory_staging(emu):
+    """Every pass's ops and layouts, and its gate fragments where they fit, are copied
+    into shared memory beside the 64 KiB tile: the largest copy stays within two CTAs per
+    SM, the n=30 headline circuit stages every pass, and the n=12 depth-40 circuit (run on
+    the GPU by test_pair_engine_pass_with_gates_beyond_shared_memory) has a pass whose
+    gates stay in global memory."""
+    def stats(n, depth):
+        g = circuits.random_matching_circuit(n, depth, seed=1)
+        st = np.zeros(8, dtype=np.uint64)
+        rc = emu.emu_pairs_stats(ctypes.c_uint32(n), ctypes.c_void_p(g.ctypes.data), ctypes.c_size_t(len(g)),
+                                 ctypes.c_void_p(st.ctypes.data))
+        assert rc == 0
+        return st
+    tile = 16 << 12
+    for n, depth in ((12, 40), (20, 40), (30, 40)):
+        st = stats(n, depth)
+        assert tile + int(st[5]) <= 112 * 1024
+    assert stats(30, 40)[4] == 0
+    assert stats(12, 40)[4] >= 1
