@@ -51,6 +51,7 @@ __device__ __forceinline__ double block_sum(double v, double* red)
 // block-reduced sum per tile and slot in `partial` (row = slot, column = tile).
 constexpr int AT_M = 10;                  // 1,024 amplitudes of psi and of lambda: 32 KiB
 constexpr int AT_THREADS = 256;
+constexpr int AT_MAX_LSLOTS = 128;   // derivative slots of one pass at most (a pass with more is split)
 
 enum { AT_C1 = 0, AT_DIAG = 1, AT_CX = 2 };
 
@@ -63,7 +64,7 @@ struct AdjTileOp {
     uint8_t tile_bit;  // tile-index bit of a tile-bit qubit
     uint8_t pad[2];
     int32_t slot;      // first derivative slot
-    int32_t pad2;
+    int32_t lslot;     // its first slot among the pass's slots
     double m[8];       // the inverse op: C1 2x2, or d0, d1 for DIAG
     double dm[3][8];   // derivative matrices, C1 layout
 };
@@ -73,18 +74,24 @@ struct AdjTilePass {
     uint8_t nonlocal_q[64];
     uint64_t g_lo[64];         // local index bits 0-5 -> global offset
     uint64_t g_hi[32];         // local index bits 6-10 -> global offset
-    int32_t n_nonlocal, op_begin, op_end, pad;
+    int32_t n_nonlocal, op_begin, op_end;
+    int32_t n_lslots;          // derivative slots of the pass's ops
+    int32_t lslot_begin;       // their global slot numbers: lslots[lslot_begin + local slot]
+    int32_t pad[3];
 };
 static_assert(sizeof(AdjTilePass) % 16 == 0, "AdjTilePass layout");
 
 __global__ void __launch_bounds__(AT_THREADS, 3)
 k_adj_tiles(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTilePass* __restrict__ passes,
-            int pass_index, const AdjTileOp* __restrict__ ops, int M, uint64_t tiles,
-            double* __restrict__ partial)
+            int pass_index, const AdjTileOp* __restrict__ ops, const int32_t* __restrict__ lslots, int M,
+            uint64_t tiles, double* __restrict__ partial)
 {
+    // shared memory: the psi and lambda tiles, then each warp's derivative sums per slot
+    // of the pass (reduced over the warps once per tile)
     extern __shared__ __align__(16) double2 at_sm[];
     __shared__ AdjTilePass P;
-    __shared__ double red[AT_THREADS / 32];
+    constexpr int WARPS = AT_THREADS / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     {
         const uint4* src = reinterpret_cast<const uint4*>(passes + pass_index);
         uint4* dst = reinterpret_cast<uint4*>(&P);
@@ -94,6 +101,7 @@ k_adj_tiles(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTileP
     const uint32_t T = 1u << M;
     double2* sp = at_sm;
     double2* sl = at_sm + T;
+    double* wsum = reinterpret_cast<double*>(at_sm + 2 * T);      // [local slot][warp]
     for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         uint64_t base = 0;
         for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
@@ -107,7 +115,7 @@ k_adj_tiles(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTileP
             const AdjTileOp& op = ops[o];
             const uint4 hdr = __ldg(reinterpret_cast<const uint4*>(&op));
             const int kind = hdr.x & 0xFFu, p = (hdr.x >> 8) & 0xFFu, flags = hdr.x >> 24;
-            const int nd = hdr.y & 0xFFu, tbit = (hdr.y >> 8) & 0xFFu, slot = (int)hdr.z;
+            const int nd = hdr.y & 0xFFu, tbit = (hdr.y >> 8) & 0xFFu, lslot = (int)hdr.w;
             Coef<double> inv;
             {
                 const double2* m2 = reinterpret_cast<const double2*>(op.m);
@@ -149,8 +157,10 @@ k_adj_tiles(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTileP
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
                     if (d >= nd) break;
-                    const double v = block_sum(acc[d], red);
-                    if (threadIdx.x == 0) partial[(uint64_t)(slot + d) * tiles + tile] = v;
+                    double v = acc[d];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0) wsum[(lslot + d) * WARPS + warp] = v;
                 }
             } else if (kind == AT_DIAG) {
                 const bool tile_bit = flags & 1;
@@ -192,6 +202,14 @@ k_adj_tiles(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTileP
             const uint64_t g = base + P.g_lo[l & 63u] + P.g_hi[l >> 6];
             psi[g] = sp[l];
             lam[g] = sl[l];
+        }
+        // the tile's derivative sums, warps added in a fixed order (the barrier after the
+        // last op made every warp's sums visible)
+        for (int j = threadIdx.x; j < P.n_lslots; j += AT_THREADS) {
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < WARPS; w++) v += wsum[j * WARPS + w];
+            partial[(uint64_t)lslots[P.lslot_begin + j] * tiles + tile] = v;
         }
         __syncthreads();
     }
@@ -507,6 +525,8 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
     // qubits; a pass never spans a checkpoint, after which psi is reloaded
     std::vector<AdjTilePass> tpasses;
     std::vector<AdjTileOp> tops;
+    std::vector<int32_t> tslots;                      // per pass: global slot of each local slot
+    int max_lslots = 0;
     struct Seg { size_t pass_end; int ck; };          // reload checkpoint ck after the passes
     std::vector<Seg> segs;
     {
@@ -548,6 +568,7 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
                     for (int b2 = 0; b2 < 5 && 6 + b2 < TM; b2++)
                         if ((j >> b2) & 1) P.g_hi[j] |= 1ull << local_q[6 + b2];
                 P.op_begin = (int32_t)tops.size();
+                P.lslot_begin = (int32_t)tslots.size();
                 for (int i : idx) {
                     const EOp& e = rev[i];
                     const size_t kk = orig[i];
@@ -564,16 +585,30 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
                         if (pos[e.q] >= 0) t.p = (uint8_t)pos[e.q];
                         else { t.flags |= 1; t.tile_bit = (uint8_t)tbit[e.q]; }
                     } else {
+                        if ((int)(tslots.size() - P.lslot_begin) + n_slot[kk] > AT_MAX_LSLOTS) {
+                            // the warps' sums would not fit: the rest of the ops in a second
+                            // pass over the same layout
+                            P.op_end = (int32_t)tops.size();
+                            P.n_lslots = (int32_t)tslots.size() - P.lslot_begin;
+                            max_lslots = std::max(max_lslots, P.n_lslots);
+                            tpasses.push_back(P);
+                            P.op_begin = (int32_t)tops.size();
+                            P.lslot_begin = (int32_t)tslots.size();
+                        }
                         t.kind = AT_C1;
                         t.p = (uint8_t)pos[e.q];
                         std::memcpy(t.m, e.m, sizeof(t.m));
                         t.nd = (uint8_t)n_slot[kk];
                         t.slot = first_slot[kk];
+                        t.lslot = (int32_t)tslots.size() - P.lslot_begin;
+                        for (int d = 0; d < n_slot[kk]; d++) tslots.push_back(first_slot[kk] + d);
                         for (int d = 0; d < n_slot[kk]; d++) deriv_matrix(eops[kk], slots[first_slot[kk] + d].i, t.dm[d]);
                     }
                     tops.push_back(t);
                 }
                 P.op_end = (int32_t)tops.size();
+                P.n_lslots = (int32_t)tslots.size() - P.lslot_begin;
+                max_lslots = std::max(max_lslots, P.n_lslots);
                 tpasses.push_back(P);
                 return std::vector<int>{};
             });
@@ -586,6 +621,11 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
         return fail(err, "cudaMalloc(reverse plan)");
     if ((err = grow(A.rev_ops, std::max<size_t>(1, tops.size()) * sizeof(AdjTileOp))) != cudaSuccess)
         return fail(err, "cudaMalloc(reverse plan)");
+    if ((err = grow(A.rev_slots, std::max<size_t>(1, tslots.size()) * sizeof(int32_t))) != cudaSuccess)
+        return fail(err, "cudaMalloc(reverse plan)");
+    if (!tslots.empty() && (err = cudaMemcpyAsync(A.rev_slots.p, tslots.data(), tslots.size() * sizeof(int32_t),
+                                                  cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(err, "reverse plan upload");
     if (!tpasses.empty() && (err = cudaMemcpyAsync(A.rev_passes.p, tpasses.data(), tpasses.size() * sizeof(AdjTilePass),
                                                    cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(err, "reverse plan upload");
@@ -595,7 +635,8 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
     double2* psi = static_cast<double2*>(s->state);
     {
         static int ctas_per_sm = 0, sms = 0;
-        const size_t smem = 2 * sizeof(double2) << AT_M;
+        // the tiles and the warps' sums of up to AT_MAX_LSLOTS slots of a pass
+        const size_t smem = (2 * sizeof(double2) << AT_M) + AT_MAX_LSLOTS * (AT_THREADS / 32) * sizeof(double);
         if (ctas_per_sm == 0) {
             if ((err = cudaFuncSetAttribute(k_adj_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
                     cudaSuccess ||
@@ -606,13 +647,14 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
             ctas_per_sm = std::max(ctas_per_sm, 1);
         }
         const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)ctas_per_sm * sms);
-        const size_t dyn = 2 * sizeof(double2) << TM;
+        const size_t dyn = (2 * sizeof(double2) << TM) + (size_t)max_lslots * (AT_THREADS / 32) * sizeof(double);
         size_t pi = 0;
         for (const Seg& sg : segs) {
             for (; pi < sg.pass_end; pi++)
                 k_adj_tiles<<<grid, AT_THREADS, dyn>>>(psi, lam, static_cast<const AdjTilePass*>(A.rev_passes.p),
-                                                       (int)pi, static_cast<const AdjTileOp*>(A.rev_ops.p), TM,
-                                                       tiles, partial);
+                                                       (int)pi, static_cast<const AdjTileOp*>(A.rev_ops.p),
+                                                       static_cast<const int32_t*>(A.rev_slots.p), TM, tiles,
+                                                       partial);
             if ((err = cudaGetLastError()) != cudaSuccess) return fail(err, "reverse pass");
             // psi is now the state before op ckpt_at[ck]: reload the stored copy
             if (sg.ck >= 0 &&

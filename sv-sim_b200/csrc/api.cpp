@@ -230,6 +230,7 @@ void free_adjoint_scratch(AdjScratch& a)
     release(a.plan_ops);
     release(a.rev_passes);
     release(a.rev_ops);
+    release(a.rev_slots);
     for (GrowBuf& b : a.ckpts) release(b);
     a.ckpts.clear();
 }

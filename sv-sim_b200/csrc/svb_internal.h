@@ -366,7 +366,7 @@ void release(GrowBuf& b);
 struct AdjScratch {
     GrowBuf lam, partial, results, terms, final_state;
     GrowBuf plan_passes, plan_stages, plan_ops;     // forward segments' staged plans
-    GrowBuf rev_passes, rev_ops;                    // the tiled reverse sweep's plan
+    GrowBuf rev_passes, rev_ops, rev_slots;         // the tiled reverse sweep's plan
     std::vector<GrowBuf> ckpts;
 };
 
