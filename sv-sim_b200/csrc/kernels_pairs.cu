@@ -10,8 +10,9 @@
 // entries of the real 8x8 form G'), and the 2 accumulator registers a thread gets back are
 // the real and imaginary part of its own output amplitude a' = t & 3.  So the tile never
 // leaves the registers between blocks on the same pair.  A PO_SWAP exchanges a lane bit
-// with a register bit by one warp shuffle per moved word; a PO_RELAYOUT sends the tile
-// through shared memory with the staged engine's XOR swizzle.
+// with a register bit by one warp shuffle per moved word; a PO_LPERM permutes the lane
+// bits by one indexed shuffle of every word; a PO_RELAYOUT sends the tile through shared
+// memory with the staged engine's XOR swizzle.
 #include "staged_core.cuh"
 
 namespace svb {
@@ -158,6 +159,17 @@ k_pairs(double2* __restrict__ sv, const PairPass* __restrict__ passes, const Pai
                 }
             } else if (op.kind == PO_SWAP) {
                 swap_any(v, op.lane, op.reg);
+            } else if (op.kind == PO_LPERM) {
+                // lane bit b takes the element of lane bit from[b]: read every register
+                // from the lane whose bit from[b] is this lane's bit b
+                int src = 0;
+#pragma unroll
+                for (int b = 0; b < PR_LANE_BITS; b++) src |= ((lane >> b) & 1) << ((op.gate >> (3 * b)) & 7u);
+#pragma unroll
+                for (int k = 0; k < PR_NR; k++) {
+                    v[k].x = __shfl_sync(0xffffffffu, v[k].x, src);
+                    v[k].y = __shfl_sync(0xffffffffu, v[k].y, src);
+                }
             } else {
                 Slots from, to;
                 make_slots<double, PR_TILE_BITS - RB>(slay[op.src - P.load_layout], tid, from);

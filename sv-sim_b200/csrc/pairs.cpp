@@ -18,11 +18,15 @@
 // pending matrix first.
 //
 // Each block needs its two qubits on lane bits 0 and 1.  The layout planner follows the
-// blocks: a qubit held in a register bit is swapped onto the lane with one warp shuffle
-// exchange (PO_SWAP), a qubit on another lane goes through a register (two exchanges), and
-// a qubit on a warp bit needs a shared-memory redistribution (PO_RELAYOUT) whose new
+// blocks: a qubit held in a register bit is swapped onto a lane with one warp shuffle
+// exchange (PO_SWAP: selects around the shuffles), qubits on other lanes are brought to
+// lanes 0 and 1 by one permutation of the lane bits (PO_LPERM: one indexed shuffle per
+// word, no selects), and a qubit on a warp bit needs a shared-memory redistribution
+// (PO_RELAYOUT) whose new
 // layout keeps the soonest-needed qubits on lanes and registers.  A pass is loaded and
-// stored with its 5 lowest local positions on the lanes (coalesced 128-byte runs).
+// stored with its 3 lowest local positions (qubits 0..2) on lanes, which makes every warp
+// access whole 128-byte runs; the load puts the first block's qubits on lanes 0 and 1 and
+// the next-needed qubits in registers.
 //
 // The device form of a block variant is its real 8x8 matrix G'[r][kk] with rows
 // r = 2a' + re/im of the output amplitude and columns kk = a (real part) or 4 + a
@@ -323,25 +327,36 @@ struct LayoutPlanner {
         plan.ops.push_back(op);
         plan.n_relayouts++;
     }
-    // the register whose qubit is needed last
-    int spare_reg(const std::vector<int>& next_use) const
+    // one permutation of the lane bits: lane bit b receives what lane bit from[b] held
+    void lane_perm(const int* from)
     {
-        int best = 0;
-        for (int r = 1; r < RB; r++)
-            if (next_use[slot_pos[SLOT_REG + r]] > next_use[slot_pos[SLOT_REG + best]]) best = r;
-        return best;
-    }
-    void move_to_lane(int pos, int lane, const std::vector<int>& next_use)
-    {
-        const int s = where[pos];
-        if (s == lane) return;
-        if (s >= SLOT_REG && s < SLOT_WARP) {
-            swap_lr(lane, s - SLOT_REG);
-            return;
+        int old[PR_LANE_BITS];
+        for (int b = 0; b < PR_LANE_BITS; b++) old[b] = slot_pos[b];
+        uint32_t code = 0;
+        for (int b = 0; b < PR_LANE_BITS; b++) {
+            code |= (uint32_t)from[b] << (3 * b);
+            slot_pos[b] = old[from[b]];
+            where[slot_pos[b]] = b;
         }
-        const int r = spare_reg(next_use);      // another lane: through a register
-        swap_lr(s, r);
-        swap_lr(lane, r);
+        if (!dry) {
+            PairOp op;
+            std::memset(&op, 0, sizeof(op));
+            op.kind = PO_LPERM;
+            op.gate = code;
+            plan.ops.push_back(op);
+            plan.n_lane_perms++;
+        }
+    }
+    // the lane (other than those holding x and y) whose qubit is needed last
+    int spare_lane(int x, int y, int pref, const std::vector<int>& next_use) const
+    {
+        if (slot_pos[pref] != x && slot_pos[pref] != y) return pref;
+        int best = -1;
+        for (int l = 0; l < PR_LANE_BITS; l++) {
+            if (slot_pos[l] == x || slot_pos[l] == y) continue;
+            if (best < 0 || next_use[slot_pos[l]] > next_use[slot_pos[best]]) best = l;
+        }
+        return best;
     }
     // a layout with x, y on lanes 0, 1 and the other positions by next use
     void relayout_for(int x, int y, const std::vector<int>& next_use)
@@ -369,20 +384,20 @@ struct LayoutPlanner {
         for (int w = SLOT_WARP; w < NSLOT; w++) sp[w] = rest[k++];
         relayout(sp);
     }
-    // exchanges needed to bring `pos` onto a target lane (a warp bit: a relayout)
-    int cost_of(int pos) const
-    {
-        const int s = where[pos];
-        if (s <= 1) return 0;
-        if (s >= SLOT_REG && s < SLOT_WARP) return 1;
-        if (s < SLOT_REG) return 2;
-        return 8;
-    }
+    // cost of bringing x and y to lanes 0 and 1, in units of about one lane permutation:
+    // a lane/register exchange is four, a relayout fourteen
     int pair_cost(int x, int y) const
     {
         const int sx = where[x], sy = where[y];
         if ((sx == 0 && sy == 1) || (sx == 1 && sy == 0)) return 0;
-        return cost_of(x) + cost_of(y);
+        if (sx >= SLOT_WARP || sy >= SLOT_WARP) return 14;
+        int c = 0;
+        bool perm = false;
+        for (int s : {sx, sy}) {
+            if (s >= SLOT_REG) c += 4;
+            else if (s > 1) perm = true;
+        }
+        return c + (perm ? 1 : 0);
     }
     void ensure(int x, int y, const std::vector<int>& next_use)
     {
@@ -392,9 +407,22 @@ struct LayoutPlanner {
             relayout_for(x, y, next_use);
             return;
         }
-        if (sy == 0 || sx == 1) std::swap(x, y);
-        move_to_lane(x, 0, next_use);
-        move_to_lane(y, 1, next_use);
+        // qubits in registers onto lanes (lane 0 for x, lane 1 for y, where free)
+        if (where[x] >= SLOT_REG) swap_lr(spare_lane(x, y, 0, next_use), where[x] - SLOT_REG);
+        if (where[y] >= SLOT_REG) swap_lr(spare_lane(x, y, 1, next_use), where[y] - SLOT_REG);
+        const int lx = where[x], ly = where[y];
+        if ((lx == 0 && ly == 1) || (lx == 1 && ly == 0)) return;
+        // then one lane permutation: a qubit already on lane 0 or 1 stays there
+        int tx = 0, ty = 1;
+        if (lx <= 1) { tx = lx; ty = 1 - lx; }
+        else if (ly <= 1) { ty = ly; tx = 1 - ly; }
+        int cur[PR_LANE_BITS];                  // cur[b]: the old lane bit now on lane bit b
+        for (int b = 0; b < PR_LANE_BITS; b++) cur[b] = b;
+        auto exch = [&](int a, int b) { std::swap(cur[a], cur[b]); };
+        auto lane_of = [&](int old) { for (int b = 0; b < PR_LANE_BITS; b++) if (cur[b] == old) return b; return -1; };
+        if (lx != tx) exch(tx, lane_of(lx));
+        if (lane_of(ly) != ty) exch(ty, lane_of(ly));
+        lane_perm(cur);
     }
 };
 
@@ -428,7 +456,7 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
         if (e.form == F_SRN) return false;      // only real-linear: not a matrix
         if (e.form == F_M4 && (!mats || e.mat < 0 || (size_t)e.mat >= mats->size())) return false;
     }
-    select_passes(ops, n, PR_TILE_BITS, 3, [&](uint64_t L, const std::vector<int>& taken) {
+    select_passes(ops, n, PR_TILE_BITS, PR_COAL_BITS, [&](uint64_t L, const std::vector<int>& taken) {
         PairPass P;
         std::memset(&P, 0, sizeof(P));
         int pos_of[64];
@@ -475,11 +503,24 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
         }
         LayoutPlanner lp{plan, {}, {}};
         int sp[NSLOT];
-        for (int l = 0; l < PR_LANE_BITS; l++) sp[l] = l;     // the 5 lowest positions on lanes
-        std::vector<int> rest;
-        for (int p = PR_LANE_BITS; p < NSLOT; p++) rest.push_back(p);
-        std::stable_sort(rest.begin(), rest.end(), [&](int a, int b) { return next[0][a] < next[0][b]; });
-        for (int k = 0; k < (int)rest.size(); k++) sp[SLOT_REG + k] = rest[k];
+        {
+            // lanes 0 and 1: the first block's qubits; the low positions 0..2 on lanes;
+            // then the soonest-needed positions in registers, the next on the free lanes
+            // and the latest on the warp bits
+            std::vector<int> lanes;
+            if (nb > 0) { lanes.push_back(pp.blocks[0].x); lanes.push_back(pp.blocks[0].y); }
+            for (int p = 0; p < PR_COAL_BITS; p++)
+                if (std::find(lanes.begin(), lanes.end(), p) == lanes.end()) lanes.push_back(p);
+            std::vector<int> rest;
+            for (int p = 0; p < NSLOT; p++)
+                if (std::find(lanes.begin(), lanes.end(), p) == lanes.end()) rest.push_back(p);
+            std::stable_sort(rest.begin(), rest.end(), [&](int a, int b) { return next[0][a] < next[0][b]; });
+            size_t k = 0;
+            for (int r = 0; r < RB; r++) sp[SLOT_REG + r] = rest[k++];
+            while ((int)lanes.size() < PR_LANE_BITS) lanes.push_back(rest[k++]);
+            for (int l = 0; l < PR_LANE_BITS; l++) sp[l] = lanes[l];
+            for (int w = SLOT_WARP; w < NSLOT; w++) sp[w] = rest[k++];
+        }
         lp.set(sp);
         P.load_layout = lp.push_layout();
         P.op_begin = (int32_t)plan.ops.size();
@@ -533,24 +574,21 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
             plan.ops.push_back(op);
             plan.n_blocks++;
         }
-        // 3. back to a storable layout: the 5 lowest positions on the lanes
+        // 3. back to a storable layout: positions 0..2 on lanes
         bool warp_low = false;
-        for (int p = 0; p < PR_LANE_BITS; p++)
+        for (int p = 0; p < PR_COAL_BITS; p++)
             if (lp.where[p] >= SLOT_WARP) warp_low = true;
         if (warp_low) {
-            int canon[NSLOT];
-            std::memcpy(canon, sp, sizeof(canon));
-            lp.relayout(canon);
+            lp.relayout(sp);                   // the load layout is storable
         } else {
-            for (int l = 0; l < PR_LANE_BITS; l++) {
-                if (lp.slot_pos[l] < PR_LANE_BITS) continue;
-                for (int p = 0; p < PR_LANE_BITS; p++) {
-                    const int s = lp.where[p];
-                    if (s >= SLOT_REG && s < SLOT_WARP) {
+            for (int p = 0; p < PR_COAL_BITS; p++) {
+                const int s = lp.where[p];
+                if (s < SLOT_REG) continue;    // on a lane already
+                for (int l = 0; l < PR_LANE_BITS; l++)
+                    if (lp.slot_pos[l] >= PR_COAL_BITS) {
                         lp.swap_lr(l, s - SLOT_REG);
                         break;
                     }
-                }
             }
         }
         P.store_layout = lp.push_layout();

@@ -132,12 +132,17 @@ void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& p
 // bits, described by a DevStage (thr_pos[0..4] = lane bits, thr_pos[5..7] = warp bits,
 // reg_pos = register bits).  A block is a 4x4 complex matrix on the two qubits held by
 // lane bits 0 and 1 (amplitude index a = lane bits 0 + 2 lane bit 1), applied with
-// mma.sync m8n8k4 f64 to every register slot.  Between blocks, lane and register bits
-// are exchanged with warp shuffles, or the tile is redistributed through shared memory.
+// mma.sync m8n8k4 f64 to every register slot.  Between blocks, a lane bit and a register
+// bit are exchanged with warp shuffles (PO_SWAP), the lane bits are permuted by one
+// indexed shuffle of every register (PO_LPERM), or the tile is redistributed through
+// shared memory (PO_RELAYOUT).
 constexpr int PR_TILE_BITS = 12;
 constexpr int PR_LANE_BITS = 5;
+// qubits 0..2 are local in every pass (positions 0..2) and sit on lane bits when a tile is
+// loaded and stored, so that every warp access is made of whole 128-byte runs
+constexpr int PR_COAL_BITS = 3;
 constexpr int PR_MAX_COND = 2;          // tile-selected variants: at most 2 non-local qubits
-enum PairOpKind : uint8_t { PO_SWAP = 0, PO_RELAYOUT = 1, PO_BLOCK = 2 };
+enum PairOpKind : uint8_t { PO_SWAP = 0, PO_RELAYOUT = 1, PO_BLOCK = 2, PO_LPERM = 3 };
 
 struct PairOp {                          // 16 bytes
     uint8_t kind;
@@ -146,7 +151,9 @@ struct PairOp {                          // 16 bytes
     uint8_t ncond;                       // PO_BLOCK: number of condition qubits
     uint8_t cond_q[PR_MAX_COND];         // PO_BLOCK: global qubits selecting the variant
     uint16_t layout;                     // PO_RELAYOUT: target layout
-    uint32_t gate;                       // PO_BLOCK: first variant (units of 32 double2)
+    uint32_t gate;                       // PO_BLOCK: first variant (units of 32 double2);
+                                         // PO_LPERM: 3 bits per lane bit b, the lane bit
+                                         // whose element moves to lane bit b
     uint16_t src;                        // PO_RELAYOUT: current layout
     uint16_t pad;
 };
@@ -177,7 +184,7 @@ struct PairPlan {
     std::vector<PairOp> ops;
     std::vector<DevStage> layouts;
     std::vector<double> gates;           // per variant: 32 lanes x (B0, B1)
-    size_t n_blocks = 0, n_swaps = 0, n_relayouts = 0;
+    size_t n_blocks = 0, n_swaps = 0, n_relayouts = 0, n_lane_perms = 0;
     size_t stage_bytes = 0;              // largest per-pass copy into shared memory
 };
 

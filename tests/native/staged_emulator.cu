@@ -307,8 +307,14 @@ extern "C" int emu_pairs_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
         };
         const DevStage& Ld = plan.layouts[P.load_layout];
         const DevStage& St = plan.layouts[P.store_layout];
-        for (int l = 0; l < PR_LANE_BITS; l++)
-            if (St.thr_pos[l] >= PR_LANE_BITS) return -5;     // store lanes must be the low positions
+        for (int p = 0; p < PR_COAL_BITS; p++) {              // positions 0..2 on lanes at load and store
+            bool ld = false, st = false;
+            for (int l = 0; l < PR_LANE_BITS; l++) {
+                ld |= Ld.thr_pos[l] == p;
+                st |= St.thr_pos[l] == p;
+            }
+            if (!ld || !st) return -5;
+        }
         for (uint64_t tile = 0; tile < tiles; tile++) {
             uint64_t base = 0;
             for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
@@ -344,6 +350,21 @@ extern "C" int emu_pairs_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
                         }
                     }
                     std::swap(slot_pos[L], slot_pos[PR_LANE_BITS + R]);
+                } else if (op.kind == PO_LPERM) {
+                    // lane bit b takes the element of lane bit from[b]
+                    int from[PR_LANE_BITS];
+                    for (int b = 0; b < PR_LANE_BITS; b++) from[b] = (int)((op.gate >> (3 * b)) & 7u);
+                    std::vector<double2> old(regs);
+                    for (int t = 0; t < NT; t++) {
+                        const int lane = t & 31;
+                        int src = 0;
+                        for (int b = 0; b < PR_LANE_BITS; b++) src |= ((lane >> b) & 1) << from[b];
+                        if (src > 31) return -7;
+                        for (int k = 0; k < NR; k++) regs[(size_t)t * NR + k] = old[(size_t)((t & ~31) | src) * NR + k];
+                    }
+                    int sp[PR_LANE_BITS];
+                    for (int b = 0; b < PR_LANE_BITS; b++) sp[b] = slot_pos[from[b]];
+                    for (int b = 0; b < PR_LANE_BITS; b++) slot_pos[b] = sp[b];
                 } else if (op.kind == PO_RELAYOUT) {
                     const DevStage& A = plan.layouts[op.src];
                     const DevStage& B = plan.layouts[op.layout];
@@ -435,6 +456,7 @@ extern "C" int emu_pairs_stats(uint32_t n, const svb_gate* gates, size_t n_gates
     for (const PairPass& P : plan.passes) unstaged += P.stage_gates ? 0 : 1;
     stats[4] = unstaged;
     stats[5] = plan.stage_bytes;
+    stats[6] = plan.n_lane_perms;
     return 0;
 }
 

@@ -352,11 +352,11 @@ def test_pair_engine_random_matching_vs_oracle(oracle, n):
 
 
 def test_pair_engine_pass_with_gates_beyond_shared_memory(oracle):
-    """n = 12, depth 40: one pass holds more gate fragments than fit beside the tile in
+    """n = 12, depth 60: two passes hold more gate fragments than fit beside the tile in
     shared memory (tests/test_plan.py checks that the plan says so), so the kernel reads
-    that pass's gates from global memory."""
+    those passes' gates from global memory."""
     nat = native()
-    g = circuits.random_matching_circuit(12, 40, seed=1)
+    g = circuits.random_matching_circuit(12, 60, seed=1)
     ore, oim = oracle.run(12, g)
     _, re, im = run_gpu(12, g, nat.ENGINE_PAIRS)
     assert_close(re, im, ore, oim)

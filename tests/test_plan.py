@@ -186,7 +186,7 @@ def test_pair_plan_rejects_srn_and_small_states(emu):
 def test_pair_plan_shared_memory_staging(emu):
     """Every pass's ops and layouts, and its gate fragments where they fit, are copied
     into shared memory beside the 64 KiB tile: the largest copy stays within two CTAs per
-    SM, the n=30 headline circuit stages every pass, and the n=12 depth-40 circuit (run on
+    SM, the n=30 headline circuit stages every pass, and the n=12 depth-60 circuit (run on
     the GPU by test_pair_engine_pass_with_gates_beyond_shared_memory) has a pass whose
     gates stay in global memory."""
     def stats(n, depth):
@@ -197,8 +197,8 @@ def test_pair_plan_shared_memory_staging(emu):
         assert rc == 0
         return st
     tile = 16 << 12
-    for n, depth in ((12, 40), (20, 40), (30, 40)):
+    for n, depth in ((12, 60), (20, 40), (30, 40)):
         st = stats(n, depth)
         assert tile + int(st[5]) <= 112 * 1024
     assert stats(30, 40)[4] == 0
-    assert stats(12, 40)[4] >= 1
+    assert stats(12, 60)[4] >= 1
