@@ -379,8 +379,8 @@ struct LayoutPlanner {
         rest.erase(rest.begin() + l2);
         // soonest-needed in registers (one exchange away), then lanes 3..4, warps last
         int k = 0;
-        for (int r = 0; r < RB; r++) sp[SLOT_REG + r] = rest[k++];
         for (int l = 3; l < PR_LANE_BITS; l++) sp[l] = rest[k++];
+        for (int r = 0; r < RB; r++) sp[SLOT_REG + r] = rest[k++];
         for (int w = SLOT_WARP; w < NSLOT; w++) sp[w] = rest[k++];
         relayout(sp);
     }
@@ -516,8 +516,8 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
                 if (std::find(lanes.begin(), lanes.end(), p) == lanes.end()) rest.push_back(p);
             std::stable_sort(rest.begin(), rest.end(), [&](int a, int b) { return next[0][a] < next[0][b]; });
             size_t k = 0;
-            for (int r = 0; r < RB; r++) sp[SLOT_REG + r] = rest[k++];
             while ((int)lanes.size() < PR_LANE_BITS) lanes.push_back(rest[k++]);
+            for (int r = 0; r < RB; r++) sp[SLOT_REG + r] = rest[k++];
             for (int l = 0; l < PR_LANE_BITS; l++) sp[l] = lanes[l];
             for (int w = SLOT_WARP; w < NSLOT; w++) sp[w] = rest[k++];
         }
