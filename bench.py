@@ -313,7 +313,7 @@ def run_ours(args):
         "config": {"workload": WORKLOAD, "n_qubits": nq, "depth": DEPTH, "gates": n_gates,
                    "seed": SEED, "engine": args.engine, "tile_bits": int(info.tile_bits),
                    "passes": passes, "parallelism": f"replicas x{world}",
-                   "l2": "16 GiB state > 126 MB L2: every step streams from HBM, no flush"},
+                   "l2": f"{16 << nq >> 30} GiB state > 126 MB L2: every step streams from HBM, no flush"},
         "roofline": roofline,
         "e2e": e2e,
         "clocks": clocks.summary(),
