@@ -3,11 +3,13 @@
 
 Workload (one "step"): the n=30, depth-40 random circuit — per layer U3 with U[0,2pi)
 angles on all 30 qubits, then 15 CX on a seeded random perfect matching (1,800 gates) —
-applied in FP64 to a 16 GiB state resident in HBM, through the staged engine.  The state
-(16 GiB) is far larger than the 126 MB L2, so no L2 flush is needed between steps.
+applied in FP64 to a 16 GiB state resident in HBM, through the pair engine (two-qubit
+blocks on the FP64 tensor cores).  The state (16 GiB) is far larger than the 126 MB L2, so
+no L2 flush is needed between steps.
 
 Printed (rank 0, one JSON line): gates/s over all ranks, the roofline of the dominant
-kernel (the staged tile kernel, HBM-bound), the reference CPU path timed on this box's
+kernel (`k_pairs`: HBM bytes per launch and its FP64 tensor-pipe rate beside them), the
+reference CPU path timed on this box's
 host cores, an end-to-end figure through the C ABI with host buffers, the SM clocks seen
 during the timed region, and secondary forms (per-gate FP64 sweeps, adjoint gradients).
 
