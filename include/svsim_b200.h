@@ -161,6 +161,14 @@ svb_status svb_state_device_ptr(svb_sim* sim, void** dptr, int* precision);
 svb_status svb_measure(svb_sim* sim, const double* uniforms, uint32_t shots,
                        uint64_t* out, double* prob_total);
 
+/* Simulation::measure (:359-383) itself, with a seed in place of its time(0): seeds the
+ * C library generator with srand(seed) and draws shot s as rand() / RAND_MAX, in shot
+ * order, as the reference does after srand(time(0)); then samples as svb_measure.  The
+ * same seed gives the reference's samples for the same state.  Like the reference, it
+ * reseeds the process-wide rand() sequence (not thread-safe). */
+svb_status svb_measure_seeded(svb_sim* sim, uint32_t seed, uint32_t shots, uint64_t* out,
+                              double* prob_total);
+
 /* Largest state size svb_measure_noalloc accepts. */
 #define SVB_NOALLOC_MAX_QUBITS 30
 

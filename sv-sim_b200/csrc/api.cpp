@@ -733,6 +733,17 @@ svb_status svb_measure(svb_sim* s, const double* uniforms, uint32_t shots, uint6
     return SVB_OK;
 }
 
+svb_status svb_measure_seeded(svb_sim* s, uint32_t seed, uint32_t shots, uint64_t* out, double* prob_total)
+{
+    if (!s) return invalid("svb_measure_seeded: NULL handle");
+    if (shots > 0 && !out) return invalid("svb_measure_seeded: NULL output");
+    // the reference's draws (svsim_nvgpu_sin.cuh:367-371) with the caller's seed
+    std::vector<double> u(shots);
+    srand(seed);
+    for (uint32_t i = 0; i < shots; i++) u[i] = (double)rand() / (double)RAND_MAX;
+    return svb_measure(s, u.data(), shots, out, prob_total);
+}
+
 svb_status svb_norm2(svb_sim* s, double* out)
 {
     if (!out) return invalid("svb_norm2: NULL output");

@@ -63,6 +63,7 @@ _SIGS = {
     "svb_set_state_soa": ([_vp, _dp, _dp], ctypes.c_int),
     "svb_state_device_ptr": ([_vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "svb_measure": ([_vp, _dp, ctypes.c_uint32, _u64p, _dp], ctypes.c_int),
+    "svb_measure_seeded": ([_vp, ctypes.c_uint32, ctypes.c_uint32, _u64p, _dp], ctypes.c_int),
     "svb_norm2": ([_vp, _dp], ctypes.c_int),
     "svb_expectation": ([_vp, _vp, ctypes.c_size_t, _dp], ctypes.c_int),
     "svb_adjoint": ([_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_uint32, _vp, ctypes.c_size_t, _dp, _dp],
@@ -188,6 +189,14 @@ class Handle:
         tot = ctypes.c_double()
         check(lib().svb_measure(self.ptr, dptr(u), len(u), out.ctypes.data_as(_u64p),
                                 ctypes.byref(tot)))
+        return out, tot.value
+
+    def measure_seeded(self, seed: int, shots: int):
+        """The reference's measure() with srand(seed) in place of srand(time(0))."""
+        out = np.zeros(shots, dtype=np.uint64)
+        tot = ctypes.c_double()
+        check(lib().svb_measure_seeded(self.ptr, ctypes.c_uint32(seed), shots, out.ctypes.data_as(_u64p),
+                                       ctypes.byref(tot)))
         return out, tot.value
 
     def norm2(self) -> float:

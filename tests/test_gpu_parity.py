@@ -195,6 +195,23 @@ def test_measure_matches_oracle_rule(oracle, n):
     assert abs(tot - wtot) <= 1e-12
 
 
+def test_measure_seeded_reproduces_reference_samples():
+    """svb_measure_seeded(seed) draws the reference's rand()/RAND_MAX sequence after
+    srand(seed): on the 470-gate brickwork state it returns the samples the reference's
+    own measure() gave for that seed (golden fixture), on every engine."""
+    d = load_golden("brickwork.npz")
+    seed = int(d["sample_seed"][0])
+    for engine, tile in engines_for(16):
+        h, _, _ = run_gpu(16, d["gates16"], engine, tile)
+        samples, total = h.measure_seeded(seed, 1024)
+        assert np.array_equal(samples, d["samples16"])
+        assert abs(total - d["norm16"][0]) <= 1e-12
+        again, _ = h.measure_seeded(seed, 1024)
+        assert np.array_equal(again, samples)
+    empty, _ = h.measure_seeded(seed, 0)
+    assert len(empty) == 0
+
+
 def test_norm_of_non_unitary_circuit(oracle):
     """SRN and R are not norm-preserving as coded in the reference."""
     n = 10
