@@ -1,5 +1,6 @@
-"""Batched QAOA across ranks (svsim_b200.sharding): size-balanced assignment and the
-gather of energies and gradients, run as two gloo processes on the CPU.  The per-rank
+"""Batches across ranks (svsim_b200.sharding): QAOA instances (size-balanced assignment)
+and parameter points of one circuit (even split), with the gather of energies and
+gradients, run as two gloo processes on the CPU.  The per-rank
 evaluator is a deterministic stand-in (the GPU batch itself is covered by the gpu tests),
 so these tests check the host logic: every instance evaluated exactly once, by the rank
 the assignment names, and the gathered result equal to a single-process evaluation."""
@@ -10,7 +11,7 @@ import numpy as np
 import pytest
 
 from svsim_b200 import circuits
-from svsim_b200.sharding import ShardedQaoa, assign
+from svsim_b200.sharding import ShardedAdjoint, ShardedQaoa, assign, split_even
 
 
 class FakeEvaluator:
@@ -92,3 +93,79 @@ def test_single_process_without_distributed():
     e_ref, g_ref = FakeEvaluator(insts).run(g, b)
     assert sq.world == 1 and sq.mine == list(range(5))
     assert np.array_equal(e, e_ref) and np.array_equal(grad, g_ref)
+
+
+# ---- parameter points of one circuit (ShardedAdjoint) -----------------------------------
+
+class FakePoints:
+    """E(p) = sum sin(p) + 0.5 sum p^2; grad = cos(p) + p; records the points it saw."""
+
+    def __init__(self):
+        self.seen = []
+
+    def run(self, points, gradients=True):
+        self.seen.extend(map(tuple, points))
+        e = np.sin(points).sum(axis=1) + 0.5 * (points ** 2).sum(axis=1)
+        return e, (np.cos(points) + points) if gradients else None
+
+
+def _points(m=23, n_params=7, seed=5):
+    return np.random.default_rng(seed).uniform(-np.pi, np.pi, size=(m, n_params))
+
+
+def test_split_even_covers_each_point_once():
+    for count in (0, 1, 5, 23, 64):
+        for world in (1, 2, 3, 8):
+            parts = split_even(count, world)
+            assert len(parts) == world
+            assert [i for p in parts for i in p] == list(range(count))
+            sizes = [len(p) for p in parts]
+            assert max(sizes) - min(sizes) <= 1
+
+
+def _adj_worker(rank, world, port, out_path):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    pc = circuits.hardware_efficient_ansatz(n=4, layers=1)
+    fake = FakePoints()
+    pts = _points(n_params=len(pc.params))
+    sa = ShardedAdjoint(pc, None, make_local=lambda: fake)
+    e, g = sa.run(pts)
+    e2, g2 = sa.run(pts, gradients=False)
+    np.savez(f"{out_path}.{rank}.npz", e=e, g=g, e2=e2, g2_none=np.array(g2 is None),
+             seen=np.array(fake.seen))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_adjoint_two_gloo_ranks_matches_one_process(tmp_path):
+    import torch.multiprocessing as mp
+    world = 2
+    out = str(tmp_path / "adj")
+    mp.start_processes(_adj_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn",
+                       join=True)
+    pc = circuits.hardware_efficient_ansatz(n=4, layers=1)
+    pts = _points(n_params=len(pc.params))
+    e_ref, g_ref = FakePoints().run(pts)
+    parts = split_even(len(pts), world)
+    for r in range(world):
+        d = np.load(f"{out}.{r}.npz")
+        assert np.array_equal(d["e"], e_ref) and np.array_equal(d["g"], g_ref)
+        assert np.array_equal(d["e2"], e_ref) and bool(d["g2_none"])
+        # each rank evaluated exactly its own run of points, once per call
+        mine = pts[parts[r]]
+        assert np.array_equal(d["seen"], np.concatenate([mine, mine]))
+
+
+def test_sharded_adjoint_single_process():
+    pc = circuits.hardware_efficient_ansatz(n=4, layers=1)
+    pts = _points(m=3, n_params=len(pc.params))
+    sa = ShardedAdjoint(pc, None, make_local=FakePoints)
+    e, g = sa.run(pts)
+    e_ref, g_ref = FakePoints().run(pts)
+    assert sa.world == 1
+    assert np.array_equal(e, e_ref) and np.array_equal(g, g_ref)
