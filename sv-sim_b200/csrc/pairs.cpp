@@ -24,9 +24,9 @@
 // word, no selects), and a qubit on a warp bit needs a shared-memory redistribution
 // (PO_RELAYOUT) whose new
 // layout keeps the soonest-needed qubits on lanes and registers.  A pass is loaded and
-// stored with its 3 lowest local positions (qubits 0..2) on lanes, which makes every warp
-// access whole 128-byte runs; the load puts the first block's qubits on lanes 0 and 1 and
-// the next-needed qubits in registers.
+// stored with its 2 lowest local positions (qubits 0 and 1) on lanes, which makes every
+// warp access whole 64-byte runs; the load puts the first block's qubits on lanes 0 and 1
+// and the next-needed qubits on the free lanes, then in registers.
 //
 // The device form of a block variant is its real 8x8 matrix G'[r][kk] with rows
 // r = 2a' + re/im of the output amplitude and columns kk = a (real part) or 4 + a
@@ -377,7 +377,8 @@ struct LayoutPlanner {
         if (l2 < 0) l2 = (int)rest.size() - 1;
         sp[2] = rest[l2];
         rest.erase(rest.begin() + l2);
-        // soonest-needed in registers (one exchange away), then lanes 3..4, warps last
+        // soonest-needed on lanes 3..4 (one lane permutation away, both at once), then the
+        // registers (one exchange each), warps last
         int k = 0;
         for (int l = 3; l < PR_LANE_BITS; l++) sp[l] = rest[k++];
         for (int r = 0; r < RB; r++) sp[SLOT_REG + r] = rest[k++];
@@ -504,13 +505,18 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
         LayoutPlanner lp{plan, {}, {}};
         int sp[NSLOT];
         {
-            // lanes 0 and 1: the first block's qubits; the low positions 0..2 on lanes;
-            // then the soonest-needed positions in registers, the next on the free lanes
-            // and the latest on the warp bits
+            // lanes 0 and 1: the first block's qubits (where the low positions leave room);
+            // the low positions (qubits 0 and 1) on lanes; then the soonest-needed
+            // positions on the free lanes, the next in registers, the latest on the warp bits
             std::vector<int> lanes;
-            if (nb > 0) { lanes.push_back(pp.blocks[0].x); lanes.push_back(pp.blocks[0].y); }
+            auto on_lanes = [&](int p) { return std::find(lanes.begin(), lanes.end(), p) != lanes.end(); };
+            if (nb > 0) {
+                const int x = pp.blocks[0].x, y = pp.blocks[0].y;
+                const int room = PR_LANE_BITS - PR_COAL_BITS + (x < PR_COAL_BITS) + (y < PR_COAL_BITS);
+                if (room >= 2) { lanes.push_back(x); lanes.push_back(y); }
+            }
             for (int p = 0; p < PR_COAL_BITS; p++)
-                if (std::find(lanes.begin(), lanes.end(), p) == lanes.end()) lanes.push_back(p);
+                if (!on_lanes(p)) lanes.push_back(p);
             std::vector<int> rest;
             for (int p = 0; p < NSLOT; p++)
                 if (std::find(lanes.begin(), lanes.end(), p) == lanes.end()) rest.push_back(p);
@@ -574,7 +580,7 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
             plan.ops.push_back(op);
             plan.n_blocks++;
         }
-        // 3. back to a storable layout: positions 0..2 on lanes
+        // 3. back to a storable layout: positions 0..PR_COAL_BITS-1 on lanes
         bool warp_low = false;
         for (int p = 0; p < PR_COAL_BITS; p++)
             if (lp.where[p] >= SLOT_WARP) warp_low = true;

@@ -138,9 +138,11 @@ void plan_staged(const std::vector<EOp>& ops, int n, int M, int G, StagedPlan& p
 // shared memory (PO_RELAYOUT).
 constexpr int PR_TILE_BITS = 12;
 constexpr int PR_LANE_BITS = 5;
-// qubits 0..2 are local in every pass (positions 0..2) and sit on lane bits when a tile is
-// loaded and stored, so that every warp access is made of whole 128-byte runs
-constexpr int PR_COAL_BITS = 3;
+// qubits 0 and 1 are local in every pass (positions 0 and 1) and sit on lane bits when a
+// tile is loaded and stored, so that every warp access is made of whole 64-byte runs (two
+// full 32-byte sectors).  Forcing qubit 2 as well (128-byte runs) costs more passes and
+// moves than it saves in DRAM efficiency; qubit 0 alone (32-byte runs) costs more DRAM time.
+constexpr int PR_COAL_BITS = 2;
 constexpr int PR_MAX_COND = 2;          // tile-selected variants: at most 2 non-local qubits
 enum PairOpKind : uint8_t { PO_SWAP = 0, PO_RELAYOUT = 1, PO_BLOCK = 2, PO_LPERM = 3 };
 

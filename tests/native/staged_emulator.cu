@@ -307,7 +307,7 @@ extern "C" int emu_pairs_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
         };
         const DevStage& Ld = plan.layouts[P.load_layout];
         const DevStage& St = plan.layouts[P.store_layout];
-        for (int p = 0; p < PR_COAL_BITS; p++) {              // positions 0..2 on lanes at load and store
+        for (int p = 0; p < PR_COAL_BITS; p++) {              // the low positions on lanes at load and store
             bool ld = false, st = false;
             for (int l = 0; l < PR_LANE_BITS; l++) {
                 ld |= Ld.thr_pos[l] == p;
