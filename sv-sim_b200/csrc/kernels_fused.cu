@@ -25,7 +25,7 @@
 //  * Two tiles are in flight, in two TMEM slots of 256 columns (A hi, A lo: 64 each; D:
 //    128): while the threads turn one tile's D into the next operand, the tensor core
 //    runs the other tile's MMAs.
-//  * Tiles arrive by 16-byte cp.async (the 4 lowest qubits are always local: 128-byte
+//  * Tiles arrive by 16-byte cp.async (the 3 lowest qubits are always local: 64-byte
 //    runs) into prefetch buffers some tiles ahead, each thread's copies completing on
 //    the buffer's mbarrier, and leave by 16-byte stores from the transpose buffer used
 //    as an output stage.  The layouts of both (per-run XOR swizzles the planner picks)
@@ -475,13 +475,14 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
         // ---- the data warps
         const uint32_t lane_base = (uint32_t)(quad * 32) << 16;
         // the 16-byte chunks of a thread in a tile: chunk c = tid + EPI i is piece tid & 7 of
-        // run (tid >> 3) + (EPI / 8) i (local index 16 run + 2 piece)
+        // run (tid >> 3) + (EPI / 8) i (local index 16 run + 2 piece; local position 0 is
+        // qubit 0, so a piece is two adjacent amplitudes)
         // Fixed for the pass: their global offsets within a tile, their slots in a raw
         // tile and where they sit in the output stage (with the swap of its two halves).
         uint64_t goff[CHUNKS];
         uint32_t rslot[CHUNKS], oslot[CHUNKS];
         {
-            const uint64_t g_part = P.g_lo[((tid >> 3) & 3) << 4] + 2u * (uint32_t)(tid & 7);
+            const uint64_t g_part = P.g_lo[(((tid >> 3) & 3) << 4) | ((tid & 7) << 1)];
 #pragma unroll
             for (int i = 0; i < CHUNKS; i++) {
                 const uint32_t c = (uint32_t)(tid + EPI * i);
@@ -610,7 +611,7 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
                 blk++;
                 put_rows(s, v);
             } else {
-                // the tile out in 16-byte pieces (8 threads per 128-byte run)
+                // the tile out in 16-byte pieces (4 threads per 64-byte run of the state)
                 float2* dst = sv + tile_base(tj);
 #pragma unroll
                 for (int i = 0; i < CHUNKS; i++) {

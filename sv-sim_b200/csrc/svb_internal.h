@@ -218,7 +218,9 @@ void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
 // blocks over tiles of 2^FT_TILE_BITS amplitudes (fuse.cpp, kernels_fused.cu)
 // ---------------------------------------------------------------------------------
 constexpr int FT_TILE_BITS = 12;     // 4096 FP32 amplitudes per tile (32 KiB)
-constexpr int FT_LOW_BITS = 4;       // the 4 lowest qubits are always local (128-byte runs)
+// the 3 lowest qubits are always local: tiles move in whole 64-byte runs (8 amplitudes,
+// two 32-byte sectors); forcing a fourth (128-byte runs) costs more passes than it saves
+constexpr int FT_LOW_BITS = 3;
 constexpr int FT_MAX_BLOCKS = 8;     // upper bound of fused blocks per pass
 // Shared memory of a fused CTA: a transpose buffer, an output stage and the raw-tile
 // prefetch buffers (32 KiB each), then the pass's gate operands (hi + lo planes,

@@ -210,13 +210,13 @@ extern "C" int emu_fused_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
         for (uint64_t t = 0; t < tiles; t++) {
             uint64_t base = 0;
             for (int j = 0; j < P.n_nonlocal; j++) base |= ((t >> j) & 1ull) << P.nonlocal_q[j];
-            // the raw tile: 256 runs of 16 amplitudes (local index 16 r + i)
+            // the raw tile: 256 runs of 16 local positions (local index 16 r + i)
             for (uint32_t r = 0; r < 256; r++) {
-                const uint64_t g = base + P.g_lo[(r & 3) << 4] + P.g_hi[r >> 2];
                 for (uint32_t i = 0; i < 16; i++) {
+                    const uint64_t g = base + P.g_lo[((r & 3) << 4) | i] + P.g_hi[r >> 2];
                     const uint32_t w = (16 * r + i) ^ ((uint32_t)P.raw_xor[r] << 1);
-                    raw[2 * w] = re[g + i];
-                    raw[2 * w + 1] = im[g + i];
+                    raw[2 * w] = re[g];
+                    raw[2 * w + 1] = im[g];
                 }
             }
             const FusedBlock& B0 = plan.blocks[P.block_begin];
@@ -264,15 +264,31 @@ extern "C" int emu_fused_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
                 }
             }
             for (uint32_t r = 0; r < 256; r++) {
-                const uint64_t g = base + P.g_lo[(r & 3) << 4] + P.g_hi[r >> 2];
                 for (uint32_t i = 0; i < 16; i++) {
+                    const uint64_t g = base + P.g_lo[((r & 3) << 4) | i] + P.g_hi[r >> 2];
                     const uint32_t w = (16 * r + i) ^ (uint32_t)P.out_xor[r];
-                    re[g + i] = O[2 * w];
-                    im[g + i] = O[2 * w + 1];
+                    re[g] = O[2 * w];
+                    im[g] = O[2 * w + 1];
                 }
             }
         }
     }
+    return 0;
+}
+
+// passes and blocks of a fused plan, without running it
+extern "C" int emu_fused_stats(uint32_t n, const svb_gate* gates, size_t n_gates, int k, uint64_t* n_passes,
+                               uint64_t* n_blocks)
+{
+    if ((int)n < FT_TILE_BITS || k < FT_MIN_K || k > FT_MAX_K) return -1;
+    std::vector<EOp> eops;
+    for (size_t i = 0; i < n_gates; i++)
+        if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
+    if (!fusable(eops)) return -3;
+    FusedPlan plan;
+    plan_fused(eops, (int)n, k, plan);
+    *n_passes = plan.passes.size();
+    *n_blocks = plan.blocks.size();
     return 0;
 }
 
