@@ -222,43 +222,65 @@ void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
     for (size_t i = 0; i < N; i++) inf[i] = info_of(ops[i], all);
     const uint64_t low = bit(G) - 1;
     std::vector<char> done(N, 0);
-    std::vector<int> taken;
     size_t first = 0;
-    for (;;) {
-        while (first < N && done[first]) first++;
-        if (first == N) break;
-        uint64_t L = (n == M) ? all : low;
-        int nL = (n == M) ? n : G;
+    struct Cut {
+        uint64_t L = 0;
+        int nL = 0;
+        std::vector<int> taken, entries;   // entries: taken ops that made qubits local
+    };
+    // one greedy scan from `first` in program order; op `banned` is treated as blocked
+    auto scan = [&](long banned, Cut& c) {
+        c.L = (n == M) ? all : low;
+        c.nL = (n == M) ? n : G;
+        c.taken.clear();
+        c.entries.clear();
         uint64_t blocked = 0;
-        taken.clear();
         for (size_t i = first; i < N; i++) {
             if (done[i]) continue;
             const uint64_t t = inf[i].touch;
-            if (t & blocked) {
+            if ((t & blocked) || (long)i == banned) {
                 blocked |= t;
                 if (blocked == all) break;
                 continue;
             }
             const int q = inf[i].need, q2 = inf[i].need2;
-            const int extra = (q >= 0 && !((L >> q) & 1)) + (q2 >= 0 && !((L >> q2) & 1));
+            const int extra = (q >= 0 && !((c.L >> q) & 1)) + (q2 >= 0 && !((c.L >> q2) & 1));
             if (extra > 0) {
-                if (nL + extra <= M) {
-                    if (q >= 0) L |= bit(q);
-                    if (q2 >= 0) L |= bit(q2);
-                    nL += extra;
+                if (c.nL + extra <= M) {
+                    if (q >= 0) c.L |= bit(q);
+                    if (q2 >= 0) c.L |= bit(q2);
+                    c.nL += extra;
+                    c.entries.push_back((int)i);
                 } else {
                     blocked |= t;
                     if (blocked == all) break;
                     continue;
                 }
             }
-            taken.push_back((int)i);
-            done[i] = 1;
-            if ((int)taken.size() == MAX_PASS_OPS) break;
+            c.taken.push_back((int)i);
+            if ((int)c.taken.size() == MAX_PASS_OPS) break;
         }
+    };
+    Cut best, alt;
+    for (;;) {
+        while (first < N && done[first]) first++;
+        if (first == N) break;
+        scan(-1, best);
+        // one step of local search: leaving out one of the ops that chose the local
+        // qubits (the first op excepted, so that every pass makes progress) may let the
+        // pass take more ops
+        const std::vector<int> entries = best.entries;
+        for (int e : entries) {
+            if (e == (int)first) continue;
+            scan(e, alt);
+            if (alt.taken.size() > best.taken.size()) std::swap(best, alt);
+        }
+        for (int i : best.taken) done[i] = 1;
+        uint64_t L = best.L;
+        int nL = best.nL;
         for (int q = 0; nL < M && q < n; q++)
             if (!((L >> q) & 1)) { L |= bit(q); nL++; }
-        for (int i : build(L, taken)) done[i] = 0;
+        for (int i : build(L, best.taken)) done[i] = 0;
     }
 }
 

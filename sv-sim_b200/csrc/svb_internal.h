@@ -206,10 +206,12 @@ struct DevPairBuffers {
 };
 cudaError_t launch_pair_pass(void* state, int n, int pass_index, const DevPairBuffers& b, cudaStream_t s);
 
-// The pass cut shared by the staged and pair planners: ops in program order are taken
-// into a pass of M local qubits (always including the G lowest) while their dense or CX
-// target can be made local and they touch no qubit of an op skipped earlier.  `build`
-// receives each pass's local-qubit mask and ops and returns the ops it could not place.
+// The pass cut shared by the staged, pair and adjoint planners: ops in program order are
+// taken into a pass of M local qubits (always including the G lowest) while their dense
+// or CX target can be made local and they touch no qubit of an op skipped earlier; of the
+// cuts that leave out one of the ops that brought new qubits in, the one taking the most
+// ops is kept.  `build` receives each pass's local-qubit mask and ops and returns the ops
+// it could not place.
 void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
                    const std::function<std::vector<int>(uint64_t, const std::vector<int>&)>& build);
 
