@@ -63,8 +63,9 @@ struct AdjTileOp {
     uint8_t nd;        // derivative slots (AT_C1 only)
     uint8_t tile_bit;  // tile-index bit of a tile-bit qubit
     uint8_t pad[2];
-    int32_t slot;      // first derivative slot
-    int32_t lslot;     // its first slot among the pass's slots
+    int32_t pad2;
+    int32_t lslot;     // its first derivative slot among the pass's slots (the global
+                       // slot numbers are in the pass's table)
     double m[8];       // the inverse op: C1 2x2, or d0, d1 for DIAG
     double dm[3][8];   // derivative matrices, C1 layout
 };
@@ -599,7 +600,6 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
                         t.p = (uint8_t)pos[e.q];
                         std::memcpy(t.m, e.m, sizeof(t.m));
                         t.nd = (uint8_t)n_slot[kk];
-                        t.slot = first_slot[kk];
                         t.lslot = (int32_t)tslots.size() - P.lslot_begin;
                         for (int d = 0; d < n_slot[kk]; d++) tslots.push_back(first_slot[kk] + d);
                         for (int d = 0; d < n_slot[kk]; d++) deriv_matrix(eops[kk], slots[first_slot[kk] + d].i, t.dm[d]);
