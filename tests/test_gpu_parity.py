@@ -9,7 +9,7 @@ import math
 import numpy as np
 import pytest
 
-from conftest import fidelity, load_golden
+from conftest import cx_dense_circuit, fidelity, load_golden
 from svsim_b200 import circuits, gates as G
 
 pytestmark = pytest.mark.gpu
@@ -369,11 +369,11 @@ def test_pair_engine_random_matching_vs_oracle(oracle, n):
 
 
 def test_pair_engine_pass_with_gates_beyond_shared_memory(oracle):
-    """n = 12, depth 60: two passes hold more gate fragments than fit beside the tile in
-    shared memory (tests/test_plan.py checks that the plan says so), so the kernel reads
-    those passes' gates from global memory."""
+    """The CX-dense n = 12 circuit: its passes hold more gate fragments than fit beside the
+    tile in shared memory (tests/test_plan.py checks that the plan says so), so the kernel
+    reads those passes' gates from global memory."""
     nat = native()
-    g = circuits.random_matching_circuit(12, 60, seed=1)
+    g = cx_dense_circuit()
     ore, oim = oracle.run(12, g)
     _, re, im = run_gpu(12, g, nat.ENGINE_PAIRS)
     assert_close(re, im, ore, oim)

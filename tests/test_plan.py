@@ -6,7 +6,7 @@ import math
 import numpy as np
 import pytest
 
-from conftest import fidelity
+from conftest import cx_dense_circuit, fidelity
 from svsim_b200 import circuits, gates as G
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -186,8 +186,8 @@ def test_pair_plan_rejects_srn_and_small_states(emu):
 def test_pair_plan_shared_memory_staging(emu):
     """Every pass's ops and layouts, and its gate fragments where they fit, are copied
     into shared memory beside the 64 KiB tile: the largest copy stays within two CTAs per
-    SM, the n=30 headline circuit stages every pass, and the n=12 depth-60 circuit (run on
-    the GPU by test_pair_engine_pass_with_gates_beyond_shared_memory) has a pass whose
+    SM, the n=30 headline circuit stages every pass, and the CX-dense n=12 circuit (run on
+    the GPU by test_pair_engine_pass_with_gates_beyond_shared_memory) has passes whose
     gates stay in global memory."""
     def stats(n, depth):
         g = circuits.random_matching_circuit(n, depth, seed=1)
@@ -201,4 +201,18 @@ def test_pair_plan_shared_memory_staging(emu):
         st = stats(n, depth)
         assert tile + int(st[5]) <= 112 * 1024
     assert stats(30, 40)[4] == 0
-    assert stats(12, 60)[4] >= 1
+    g = cx_dense_circuit()
+    st = np.zeros(8, dtype=np.uint64)
+    assert emu.emu_pairs_stats(ctypes.c_uint32(12), ctypes.c_void_p(g.ctypes.data), ctypes.c_size_t(len(g)),
+                               ctypes.c_void_p(st.ctypes.data)) == 0
+    assert st[4] >= 1 and tile + int(st[5]) <= 112 * 1024
+
+
+def test_pair_plan_cx_dense_vs_oracle(emu, oracle):
+    """The CX-dense circuit (passes whose gates stay in global memory) through the pair
+    plan emulator."""
+    g = cx_dense_circuit()
+    rc, re, im, _ = run_pairs_emu(emu, 12, g)
+    assert rc == 0, rc
+    ore, oim = oracle.run(12, g)
+    assert np.max(np.abs((re + 1j * im) - (ore + 1j * oim))) < 1e-13
