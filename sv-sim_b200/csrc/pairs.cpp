@@ -16,17 +16,15 @@
 // a pending matrix without conditions on qubit q moves into the next pass that acts on q
 // when q is local there (nothing in between acts on q); the others are closed in pairs.
 // (n=30 depth 40: 540 blocks instead of 654, of which 285 were such closures.)  A block
-// carries at most
-// PR_MAX_COND condition qubits (4 variants); merges that would exceed it close the
-// pending matrix first.
+// carries at most PR_MAX_COND condition qubits (4 variants); merges that would exceed it
+// close the pending matrix first.
 //
 // Each block needs its two qubits on lane bits 0 and 1.  The layout planner follows the
 // blocks: a qubit held in a register bit is swapped onto a lane with one warp shuffle
 // exchange (PO_SWAP: selects around the shuffles), qubits on other lanes are brought to
 // lanes 0 and 1 by one permutation of the lane bits (PO_LPERM: one indexed shuffle per
 // word, no selects), and a qubit on a warp bit needs a shared-memory redistribution
-// (PO_RELAYOUT) whose new
-// layout keeps the soonest-needed qubits on lanes and registers.  A pass is loaded and
+// (PO_RELAYOUT) whose new layout keeps the soonest-needed qubits on lanes and registers.  A pass is loaded and
 // stored with its 2 lowest local positions (qubits 0 and 1) on lanes, which makes every
 // warp access whole 64-byte runs; the load puts the first block's qubits on lanes 0 and 1
 // and the next-needed qubits on the free lanes, then in registers.
@@ -433,6 +431,11 @@ struct LayoutPlanner {
         auto lane_of = [&](int old) { for (int b = 0; b < PR_LANE_BITS; b++) if (cur[b] == old) return b; return -1; };
         if (lx != tx) exch(tx, lane_of(lx));
         if (lane_of(ly) != ty) exch(ty, lane_of(ly));
+        // lane 2: a qubit whose position differs mod 3 from x's and y's, when lanes 2..4
+        // hold one, so that a later relayout's shared-memory phases start conflict-free
+        auto clash = [&](int b) { const int r = slot_pos[cur[b]] % 3; return r == x % 3 || r == y % 3; };
+        for (int b = 3; b < PR_LANE_BITS && clash(2); b++)
+            if (!clash(b)) exch(2, b);
         lane_perm(cur);
     }
 };
