@@ -498,7 +498,7 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
     for (size_t c = 0; c <= ckpts.size(); c++) {
         const size_t end = c < ckpts.size() ? ckpt_at[c] : K;
         std::vector<EOp> seg(eops.begin() + begin, eops.begin() + end);
-        svb_status r2 = run_eops_staged(n, s->state, seg, nullptr, A);
+        svb_status r2 = run_eops_fp64(n, s->state, seg, nullptr, A);
         if (r2 != SVB_OK) {
             if (!keep) free_adjoint_scratch(A);
             return r2;

@@ -228,6 +228,10 @@ void free_adjoint_scratch(AdjScratch& a)
     release(a.plan_passes);
     release(a.plan_stages);
     release(a.plan_ops);
+    release(a.pair_passes);
+    release(a.pair_ops);
+    release(a.pair_layouts);
+    release(a.pair_gates);
     release(a.rev_passes);
     release(a.rev_ops);
     release(a.rev_slots);
@@ -235,8 +239,36 @@ void free_adjoint_scratch(AdjScratch& a)
     a.ckpts.clear();
 }
 
-svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st, AdjScratch& cache)
+svb_status run_eops_fp64(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st, AdjScratch& cache)
 {
+    PairPlan R;
+    if (n >= PR_TILE_BITS && plan_pairs(ops, n, R)) {
+        if (R.passes.empty()) return SVB_OK;
+        // the previous segment's kernels may still read the plan buffers: wait before reuse
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) e = grow(cache.pair_passes, R.passes.size() * sizeof(PairPass));
+        if (e == cudaSuccess) e = grow(cache.pair_ops, std::max<size_t>(1, R.ops.size()) * sizeof(PairOp));
+        if (e == cudaSuccess) e = grow(cache.pair_layouts, std::max<size_t>(1, R.layouts.size()) * sizeof(DevStage));
+        if (e == cudaSuccess) e = grow(cache.pair_gates, std::max<size_t>(2, R.gates.size()) * sizeof(double));
+        DevPairBuffers b;
+        b.passes = static_cast<PairPass*>(cache.pair_passes.p);
+        b.ops = static_cast<PairOp*>(cache.pair_ops.p);
+        b.layouts = static_cast<DevStage*>(cache.pair_layouts.p);
+        b.gates = static_cast<double*>(cache.pair_gates.p);
+        b.stage_bytes = R.stage_bytes;
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b.passes, R.passes.data(), R.passes.size() * sizeof(PairPass), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !R.ops.empty())
+            e = cudaMemcpy(b.ops, R.ops.data(), R.ops.size() * sizeof(PairOp), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !R.layouts.empty())
+            e = cudaMemcpy(b.layouts, R.layouts.data(), R.layouts.size() * sizeof(DevStage), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !R.gates.empty())
+            e = cudaMemcpy(b.gates, R.gates.data(), R.gates.size() * sizeof(double), cudaMemcpyHostToDevice);
+        for (size_t p = 0; e == cudaSuccess && p < R.passes.size(); p++)
+            e = launch_pair_pass(state, n, (int)p, b, st);
+        if (e != cudaSuccess) return cuda_fail(e, "pair run");
+        return SVB_OK;
+    }
     const int M = n >= 20 ? 12 : (n >= 12 ? 10 : n);
     if (M < 10) {
         for (const EOp& op : ops) {

@@ -379,14 +379,16 @@ void release(GrowBuf& b);
 struct AdjScratch {
     GrowBuf lam, partial, results, terms, final_state;
     GrowBuf plan_passes, plan_stages, plan_ops;     // forward segments' staged plans
+    GrowBuf pair_passes, pair_ops, pair_layouts, pair_gates;   // or their pair plans
     GrowBuf rev_passes, rev_ops, rev_slots;         // the tiled reverse sweep's plan
     std::vector<GrowBuf> ckpts;
 };
 
-// Runs elementary ops on an FP64 device state with the staged engine (per-gate for
-// n < 10), queued on `st`.  The plan is uploaded into `cache`'s buffers.
-svb_status run_eops_staged(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st,
-                           AdjScratch& cache);
+// Runs elementary ops on an FP64 device state, queued on `st`: the pair engine for
+// n >= PR_TILE_BITS, the staged engine for 10 <= n < 12 (or when an op has no matrix),
+// per-gate sweeps below.  The plan is uploaded into `cache`'s buffers.
+svb_status run_eops_fp64(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st,
+                         AdjScratch& cache);
 void free_adjoint_scratch(AdjScratch& a);
 struct Sim;
 // Validates gate records against the handle and lowers them to elementary ops (the
