@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--tile-bits", type=int, default=12)
     ap.add_argument("--engine", choices=["staged", "pairs"], default="pairs",
                     help="FP64 engine of the headline step")
-    ap.add_argument("--form", choices=["headline", "pergate", "fused", "qaoa", "capacity", "adjoint", "density"],
+    ap.add_argument("--form", choices=["headline", "pergate", "fused", "qaoa", "capacity", "adjoint", "density",
+                                       "config1"],
                     default="headline",
                     help="headline: the FP64 n=30 step (the measured line); the others run one "
                          "secondary form alone (for profiling and capacity runs)")
@@ -166,6 +167,95 @@ def cpu_reference_rate(circuit, threads):
     return {"value": len(sample) / (ms / 1e3), "unit": UNIT, "cores": threads, "kind": kind,
             "sample": f"{len(sample)} gates of layer 1 (every 3rd) at n=30, reference "
                       f"svsim_cpu_omp.hpp (64-bit IdxType build), sim() wall time {ms:.0f} ms"}
+
+
+class _DeviceArray:
+    """A device pointer seen by torch through __cuda_array_interface__ (no copy)."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def golden_parity(h):
+    """The handle's state (the n=30 circuit run once from |0..0>) against the reference's
+    own cpu_omp state of the same circuit, through tests/golden/matching_n30.npz: the
+    largest amplitude error at the fixture's 4,097 indices, the sketch estimate of
+    ||a - a_ref||^2 (>= 1 - F), and how many of the fixture's 4,096 reference-rule samples
+    svb_measure reproduces for the same draws."""
+    import torch
+    from svsim_b200 import _native as nat
+    path = os.path.join(ROOT, "tests", "golden", "matching_n30.npz")
+    if not os.path.exists(path):
+        return None
+    d = np.load(path)
+    ptr, prec = h.device_ptr()
+    t = torch.as_tensor(_DeviceArray(ptr, (1 << h.n, 2), "<f8" if prec == nat.SVB_FP64 else "<f4"),
+                        device=f"cuda:{torch.cuda.current_device()}")
+    a = torch.view_as_complex(t if prec == nat.SVB_FP64 else t.double())
+    idx = torch.from_numpy(d["idx"].astype(np.int64)).to(a.device)
+    max_abs = float(np.max(np.abs(a[idx].cpu().numpy() - (d["re_at"] + 1j * d["im_at"]))))
+    rows, seed = int(d["sketch_rows"][0]), int(d["sketch_seed"][0])
+    rng = np.random.default_rng(seed)
+    r = rng.integers(0, 2, size=(rows, 1 << 15)).astype(np.float64) * 2.0 - 1.0
+    c = rng.integers(0, 2, size=(rows, 1 << 15)).astype(np.float64) * 2.0 - 1.0
+    rt = torch.from_numpy(r).to(a.device).to(torch.complex128)
+    ct = torch.from_numpy(c).to(a.device).to(torch.complex128)
+    sk = (rt * (a.reshape(1 << 15, 1 << 15) @ ct.T).T).sum(dim=1).cpu().numpy()
+    del a, t
+    err2 = float(np.mean(np.abs(sk - d["sketch"]) ** 2))
+    samples, total = h.measure(d["uniforms"])
+    return {"reference": "svsim_cpu_omp.hpp (64-bit IdxType build) state of the same circuit, "
+                         "tests/golden/matching_n30.npz",
+            "max_abs_err_vs_reference": max_abs, "amplitudes_compared": int(d["idx"].size),
+            "infidelity_bound_vs_reference": err2,
+            "infidelity_bound_how": f"mean |c_k(a) - c_k(a_ref)|^2 over {rows} random-sign projections "
+                                    "(estimates ||a - a_ref||^2 >= 1 - F)",
+            "norm_diff_vs_reference": abs(total - float(d["norm"][0])),
+            "samples_equal_to_reference": int(np.sum(samples == d["samples"])),
+            "samples_compared": int(d["samples"].size)}
+
+
+def dropin_e2e(circuit, device, steps, world):
+    """The same metric through the reference's own Python front end: the libsvsim module
+    compiled from svsim/src/py_wrapper.cpp against the drop-in headers.  Each step is
+    upload() + run() + measure(1024), the calls a reference user makes; the gates are
+    appended once (the user's circuit construction).  sim() no longer copies the 16 GiB
+    state back, so nothing but the gate records, the plan and the samples crosses PCIe."""
+    import torch
+    lib = os.path.join(ROOT, "sv-sim_b200", "svsim_b200", "lib")
+    if not os.path.isdir(lib) or not any(f.startswith("libsvsim.") for f in os.listdir(lib)):
+        return None
+    sys.path.insert(0, lib)
+    import libsvsim
+    from svsim_b200 import gates as G
+    sim = libsvsim.Simulation(N_QUBITS, device)
+    for g in circuit:
+        op, qb = int(g["op"]), g["qb"]
+        if op == G.OP["U3"]:
+            sim.append(sim.U3(float(g["theta"]), float(g["phi"]), float(g["lam"]), int(qb[0])))
+        else:
+            sim.append(sim.CX(int(qb[0]), int(qb[1])))
+    sim.upload()
+    sim.run()
+    sim.measure(1024)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.upload()
+        sim.run()
+        res = sim.measure(1024)
+    torch.cuda.synchronize(device)
+    dt = (time.perf_counter() - t0) / steps
+    del sim
+    if world > 1:
+        t = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        dt = float(t.item())
+    return {"value": world * len(circuit) / dt, "unit": UNIT, "s_per_step": dt,
+            "h2d_bytes_per_step": int(circuit.nbytes), "d2h_bytes_per_step": int(8 * len(res) + 8),
+            "path": "libsvsim (svsim/src/py_wrapper.cpp built against the drop-in headers): "
+                    "upload() + run() + measure(1024)"}
 
 
 def run_reference_arm(args):
@@ -313,6 +403,18 @@ def run_ours(args):
            "d2h_bytes_per_step": int(samples.nbytes + 8),
            "path": "svb_set_circuit + svb_run + svb_measure(1024 shots), host buffers"}
 
+    e2e_dropin = dropin_e2e(circuit, device, e2e_steps, world) if nq == N_QUBITS else None
+    if e2e_dropin:
+        e2e["dropin"] = e2e_dropin
+
+    parity = None
+    if nq == N_QUBITS and rank == 0:
+        h.reset()
+        h.set_circuit(circuit)
+        h.run(sptr)
+        torch.cuda.synchronize(device)
+        parity = golden_parity(h)
+
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -322,6 +424,7 @@ def run_ours(args):
                    "passes": passes, "parallelism": f"replicas x{world}",
                    "l2": f"{16 << nq >> 30} GiB state > 126 MB L2: every step streams from HBM, no flush"},
         "roofline": roofline,
+        "parity": parity,
         "e2e": e2e,
         "clocks": clocks.summary(),
         "gpu_launches": int(args.steps * passes),
@@ -344,50 +447,6 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
-
-
-def fused_form(device, circuit, k=None, reps=3, n=N_QUBITS):
-    """The same circuit on an FP32 state through the fused tensor-core engine, with its
-    fidelity and largest amplitude error against the FP64 staged result."""
-    import torch
-    k = FUSION_WIDTH if k is None else k
-    from svsim_b200 import _native as nat
-    h64 = nat.Handle(n, device, nat.SVB_FP64)
-    h64.set_engine(nat.ENGINE_STAGED, 12 if n >= 20 else 0, 0)
-    h64.set_circuit(circuit)
-    h64.run()
-    h32 = nat.Handle(n, device, nat.SVB_FP32)
-    h32.set_engine(nat.ENGINE_FUSED, 0, k)
-    h32.set_circuit(circuit)
-    info = h32.plan_info()
-    h32.run()
-    h32.sync()
-    fid, maxd = h64.compare(h32)
-    norm32 = h32.norm2()
-    del h64
-    torch.cuda.empty_cache()
-    h32.run()
-    torch.cuda.synchronize(device)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
-        h32.run()
-    e1.record()
-    torch.cuda.synchronize(device)
-    h32.sync()
-    s = e0.elapsed_time(e1) / 1e3 / reps
-    peak, _ = peaks()
-    out = {"gates_per_s": len(circuit) / s, "ms_per_circuit": s * 1e3, "fusion_width": k,
-           "passes": int(info.n_passes), "hbm_gbs": info.moved_bytes / s / 1e9,
-           "hbm_frac_of_peak": info.moved_bytes / s / 1e9 / peak,
-           "one_minus_fidelity_vs_fp64": 1.0 - fid, "max_abs_amp_err_vs_fp64": maxd,
-           "norm_minus_one": norm32 - 1.0,
-           "kernel": f"k_fused<{k}>: split-TF32 tcgen05.mma, M=128, K={2 << k} in steps of 8, "
-                     f"N={4 << k} (X_hi [G_hi|G_lo]) + N={2 << k} (X_lo G_hi); A operand and "
-                     "accumulators in TMEM, two tiles in flight"}
-    del h32
-    torch.cuda.empty_cache()
-    return out
 
 
 def qaoa_form(device, count=512, precision="fp64", reps=5):
@@ -520,6 +579,8 @@ def run_form(args):
         res = adjoint_form(local)
     elif args.form == "density":
         res = density_form(local)
+    elif args.form == "config1":
+        res = config1_form(local)
     elif args.form == "pergate":
         from svsim_b200 import circuits
         res = per_gate_form(local, circuits.random_matching_circuit(args.qubits, DEPTH, seed=SEED), n=args.qubits)
@@ -536,30 +597,139 @@ def run_form(args):
 
 
 def per_gate_form(device, circuit, n=N_QUBITS):
-    """The per-gate FP64 engine (one HBM sweep per elementary op, as the reference) on
-    the first 4 layers (180 gates) of the circuit."""
+    """The per-gate FP64 engine (one HBM sweep per elementary op, as the reference) on the
+    whole circuit, timed with CUDA events, with the roofline of its two kernels: a dense
+    gate (k_eop_pairs) reads and writes the state once, a CX (k_cx) its control = 1 half."""
     import torch
     from svsim_b200 import _native as nat
     h = nat.Handle(n, device, nat.SVB_FP64)
     h.set_engine(nat.ENGINE_PER_GATE, 0, 0)
-    sub = circuit[:180]
-    h.set_circuit(sub)
+    h.set_circuit(circuit)
     info = h.plan_info()
-    h.run()
+    h.run()                                        # warm-up (first launches, clocks)
     torch.cuda.synchronize(device)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     h.run()
     e1.record()
     torch.cuda.synchronize(device)
+    h.sync()
     s = e0.elapsed_time(e1) / 1e3
-    peak, _ = peaks()
+    peak, kind = peaks()
     del h
     torch.cuda.empty_cache()
-    return {"gates_per_s": len(sub) / s, "hbm_gbs": info.moved_bytes / s / 1e9,
-            "frac_of_peak": info.moved_bytes / s / 1e9 / peak,
-            "sample": "first 4 layers (180 gates), one sweep per gate (CX: half sweep)",
-            "kernels": "k_eop_pairs / k_cx (4 pairs per thread in flight)"}
+    achieved = info.moved_bytes / s / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "per_gate_fp64_traffic.txt")
+    if os.path.exists(tfile):
+        vals = {}
+        for ln in open(tfile):
+            if "=" in ln and not ln.startswith("#"):
+                k, v = ln.split("=", 1)
+                vals[k.strip()] = float(v)
+        if n == N_QUBITS and "dense_bytes_per_launch_n30" in vals:
+            traffic = {"k_eop_pairs_dense": vals["dense_bytes_per_launch_n30"],
+                       "k_cx": vals.get("cx_bytes_per_launch_n30")}
+    sb = info.state_bytes
+    return {"gates_per_s": len(circuit) / s, "s_per_circuit": s, "gates": len(circuit),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{kind} hbm_gbs",
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_launch": {"k_eop_pairs_dense": 2 * sb, "k_cx": sb},
+                         "bytes_per_circuit": info.moved_bytes},
+            "sample": f"the whole circuit ({len(circuit)} gates), one launch per elementary gate",
+            "kernels": "k_eop_pairs / k_cx (4 pairs per thread in flight, 128-bit loads)"}
+
+
+def config1_form(device, reps=200):
+    """The reference's CPU-runnable case: n=16 brickwork, 20 layers (320 U3 + 150 CX =
+    470 gates).  The 1 MiB state stays in L2, so each engine is reported against the L2
+    copy bandwidth measured in this run; beside it the reference's cpu_sin on one core
+    and cpu_omp on every host core run the same circuit."""
+    import torch
+    from svsim_b200 import circuits, _native as nat
+    g = circuits.brickwork_circuit(16, 20, seed=1234)
+    l2 = nat.l2_copy_peak(device)
+    out = {"workload": "brickwork n=16, 20 layers, 470 gates, FP64", "l2_copy_peak_gbs": l2,
+           "l2_peak_source": "svb_l2_copy_peak: 2 x 16 MiB copy repeated in one launch, this run"}
+    gold = np.load(os.path.join(ROOT, "tests", "golden", "brickwork.npz"))
+    for name, eng in (("pairs", nat.ENGINE_PAIRS), ("staged", nat.ENGINE_STAGED), ("per_gate", nat.ENGINE_PER_GATE)):
+        h = nat.Handle(16, device, nat.SVB_FP64)
+        h.set_engine(eng, 0, 0)
+        h.set_circuit(g)
+        info = h.plan_info()
+        h.run()
+        re, im = h.get_state()
+        err = float(np.max(np.abs((re + 1j * im)[gold["idx16"]] - (gold["re16_at"] + 1j * gold["im16_at"]))))
+        for _ in range(5):
+            h.run()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            h.run()
+        e1.record()
+        torch.cuda.synchronize(device)
+        h.sync()
+        sec = e0.elapsed_time(e1) / 1e3 / reps
+        out[name] = {"gates_per_s": len(g) / sec, "us_per_circuit": sec * 1e6,
+                     "launches": int(info.n_passes), "l2_gbs": info.moved_bytes / sec / 1e9,
+                     "l2_frac": info.moved_bytes / sec / 1e9 / l2,
+                     "max_abs_err_vs_reference": err}
+        h.close()
+    try:
+        from oracle.oracle import RefBackend
+        threads = os.cpu_count() or 1
+        for kind, th, key in (("sin", 1, "reference_cpu_sin_1core"), ("omp", threads, "reference_cpu_omp_all_cores")):
+            if RefBackend.available(kind):
+                ref = RefBackend(kind)
+                ms = min(ref.simulate(16, g, threads=th, want_state=False)["sim_ms"] for _ in range(3))
+                out[key] = {"gates_per_s": len(g) / (ms / 1e3), "ms_per_circuit": ms, "cores": th}
+    except Exception as e:      # the CPU rates are reported, never required
+        out["reference_cpu_error"] = str(e)
+    return out
+
+
+def fused_form(device, circuit, k=None, reps=3, n=N_QUBITS):
+    """The same circuit on an FP32 state through the fused tensor-core engine, with its
+    infidelity bound and largest amplitude error against the reference's FP64 state
+    (golden fixture of the reference's cpu_omp)."""
+    import torch
+    k = FUSION_WIDTH if k is None else k
+    from svsim_b200 import _native as nat
+    h32 = nat.Handle(n, device, nat.SVB_FP32)
+    h32.set_engine(nat.ENGINE_FUSED, 0, k)
+    h32.set_circuit(circuit)
+    info = h32.plan_info()
+    h32.run()
+    h32.sync()
+    par = golden_parity(h32) if n == N_QUBITS else None
+    norm32 = h32.norm2()
+    h32.run()
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        h32.run()
+    e1.record()
+    torch.cuda.synchronize(device)
+    h32.sync()
+    s = e0.elapsed_time(e1) / 1e3 / reps
+    peak, _ = peaks()
+    out = {"gates_per_s": len(circuit) / s, "ms_per_circuit": s * 1e3, "fusion_width": k,
+           "passes": int(info.n_passes), "blocks": int(info.n_blocks), "hbm_gbs": info.moved_bytes / s / 1e9,
+           "hbm_frac_of_peak": info.moved_bytes / s / 1e9 / peak,
+           "norm_minus_one": norm32 - 1.0,
+           "kernel": f"k_fused<{k}>: split-TF32 tcgen05.mma, M=128, K={2 << k} in steps of 8, "
+                     f"N={4 << k} (X_hi [G_hi|G_lo]) + N={2 << k} (X_lo G_hi); A operand and "
+                     "accumulators in TMEM, two tiles in flight"}
+    if par:
+        out["one_minus_fidelity_bound_vs_reference"] = par["infidelity_bound_vs_reference"]
+        out["max_abs_amp_err_vs_reference"] = par["max_abs_err_vs_reference"]
+        out["samples_equal_to_reference"] = par["samples_equal_to_reference"]
+    del h32
+    torch.cuda.empty_cache()
+    return out
 
 
 def density_form(device, n=14, depth=10, reps=3):
@@ -626,12 +796,16 @@ def adjoint_form(device, reps=5):
 
 
 def secondary_forms(device, circuit):
-    """Per-gate FP64 sweeps on the same circuit, and adjoint gradients (n=20, 480 params)."""
+    """The other forms of the metric: per-gate FP64 sweeps and the fused FP32 tensor-core
+    engine on the same circuit, the n=16 CPU-runnable case, batched QAOA, capacity,
+    adjoint gradients (n=20, 480 params) and density matrices."""
     import torch
     from svsim_b200 import circuits, _native as nat
     forms = {}
     forms["per_gate_fp64"] = per_gate_form(device, circuit)
-    forms["fused_tc_fp32"] = fused_form(device, circuit)
+    forms["config1_n16_brickwork"] = config1_form(device)
+    for k in (4, 5):
+        forms[f"fused_tc_fp32_k{k}"] = fused_form(device, circuit, k=k)
     forms["qaoa_batch_fp64"] = qaoa_form(device, 512, "fp64")
     forms["qaoa_batch_fp32"] = qaoa_form(device, 512, "fp32")
     forms["capacity"] = capacity_form(device)

@@ -153,11 +153,14 @@ svb_status svb_state_device_ptr(svb_sim* sim, void** dptr, int* precision);
 /* ---- measurement ---------------------------------------------------------------- */
 
 /* Replaces Simulation::measure (:359-383) with the uniforms supplied by the caller
- * instead of rand(): shot s returns the j with S_j <= uniforms[s] < S_{j+1}, where
- * S is the inclusive prefix sum of |amplitude|^2 in index order, and 0 if there is
- * no such j — the reference's rule, including its default of 0.  The prefix sums
- * are FP64 and computed on the GPU (hierarchically, no 2^n scan array).
- * prob_total (may be NULL) receives S_{2^n}, the squared norm. */
+ * instead of rand(): shot s returns the j with S_j <= uniforms[s] < S_{j+1}, and 0 if
+ * there is no such j — the reference's rule, including its default of 0.  S is the
+ * reference's own prefix, bit for bit: S_0 = 0, S_{i+1} = fl(S_i + fl(fl(re_i^2) +
+ * fl(im_i^2))) summed in index order in FP64 (:362-365).  The GPU computes those
+ * sequential values exactly without a sequential pass (integer grid deltas inside a
+ * binade, IEEE adds one by one at ties and binade crossings) and without a 2^n scan
+ * array, so any uniform, including one equal to some S_j or next to it, gives the
+ * reference's sample for the same state.  prob_total (may be NULL) receives S_{2^n}. */
 svb_status svb_measure(svb_sim* sim, const double* uniforms, uint32_t shots,
                        uint64_t* out, double* prob_total);
 
@@ -179,18 +182,24 @@ svb_status svb_measure_seeded(svb_sim* sim, uint32_t seed, uint32_t shots, uint6
  * pointer on the current device: `state` (2^n_qubits interleaved amplitudes of
  * `precision`), `uniforms` and `samples` (`shots` entries each) and `prob_total` (one
  * double, may be NULL).  Work is queued on `stream`; results are valid once it completes.
- * The FP64 scratch lives in a fixed array of about 4 MiB in the library's device image,
+ * The FP64 scratch lives in a fixed array of about 4.1 MiB in the library's device image,
  * sized for n_qubits <= SVB_NOALLOC_MAX_QUBITS; larger states are rejected with
  * SVB_ERR_INVALID.  The first call on a device looks the array's address up
- * (cudaGetSymbolAddress), so make that first call before any stream capture.  All calls
- * on a device share the array: calls that overlap on the GPU race and must be serialised
- * by the caller.  Nothing needs clearing between calls (the kernels overwrite what they
- * read). */
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.  Modules
+ * load lazily by default (CUDA 12.2+): the first call also loads the module that holds
+ * the array and commits its memory, so a caller that later reserves the whole device
+ * should make one call first (shots = 0 is enough) or set CUDA_MODULE_LOADING=EAGER.
+ * All calls on a device share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Nothing needs clearing between calls (the kernels
+ * overwrite what they read). */
 svb_status svb_measure_noalloc(const void* state, uint32_t n_qubits, int precision,
                                const double* uniforms, uint32_t shots, uint64_t* samples,
                                double* prob_total, void* stream);
 
-/* Squared norm sum |a|^2 in FP64 (the value the reference checks against 1 at :379). */
+/* Squared norm sum |a|^2 in FP64, summed hierarchically (blocks of 4,096 amplitudes, then
+ * their prefix): accurate to a few ulps.  The reference's own check against 1 (:379) uses
+ * its sequential prefix total, which svb_measure returns as prob_total and which can lose
+ * ~1e-10 at 2^31 amplitudes when many probabilities are below half an ulp of the sum. */
 svb_status svb_norm2(svb_sim* sim, double* out);
 
 /* Re <psi| sum_t coef_t P_t |psi> in FP64 for a Pauli-sum observable. */
@@ -234,6 +243,26 @@ svb_status svb_dm_create(uint32_t n_qubits, int device, svb_sim** out);
  * gate).  SRN has no superoperator and is rejected. */
 svb_status svb_dm_set_circuit(svb_sim* sim, const svb_gate* gates, size_t n_gates,
                               const double* noise_kraus, uint32_t n_kraus);
+
+/* The superoperator of a one-qubit op in a density-matrix circuit, as the noise
+ * variant bakes noise into its gates (svsim_qsharp_noise/noise_gate_*.cuh tables, applied
+ * by C2_GATE, svsim_qsharp_noise/svsim_nvgpu_sin.cuh:1727-1800): `op` is the enum OP value
+ * of a one-qubit gate and m the 4x4 complex matrix e_rc, row-major, re/im interleaved,
+ * acting as out[r] = sum_c e_rc in[c] on the local index r = 2 i + j of rho[i][j] for the
+ * gate's qubit (C2_GATE's pos0..pos3 on the pair (qubit, qubit + n_qubits)).  280 bytes. */
+typedef struct svb_superop {
+    uint32_t op;
+    uint32_t reserved;
+    double m[32];
+} svb_superop;
+
+/* svb_dm_set_circuit with per-op superoperators: every gate whose op has an entry in
+ * `superops` is applied as that superoperator alone (it replaces rho -> U rho U^dagger and
+ * the Kraus noise after the gate, as the reference's noisy gates do); the other gates as
+ * in svb_dm_set_circuit. */
+svb_status svb_dm_set_circuit_superops(svb_sim* sim, const svb_gate* gates, size_t n_gates,
+                                       const double* noise_kraus, uint32_t n_kraus,
+                                       const svb_superop* superops, size_t n_superops);
 
 /* The diagonal of rho (the outcome probabilities), 2^n_qubits doubles, to the host. */
 svb_status svb_dm_probabilities(svb_sim* sim, double* out);
@@ -296,6 +325,52 @@ svb_status svb_qaoa_info(const svb_qaoa_batch* batch, svb_qaoa_stats* info);
 
 svb_status svb_qaoa_destroy(svb_qaoa_batch* batch);
 
+/* ---- batched circuits (no reference counterpart) ----------------------------------- */
+
+/* Many independent circuits, each on its own state of n_qubits[i] qubits (1..24, sizes
+ * mixed freely), run from |0..0> together by one persistent cooperative launch replayed
+ * from a CUDA graph; replaces one Simulation and one sim() per circuit
+ * (svsim_nvgpu_sin.cuh:193-339) with its fixed launch shape (:309-316, config.hpp:48).
+ * Circuit i's gates are gates[gate_offsets[i] .. gate_offsets[i+1]); its observable (may be
+ * empty) terms[term_offsets[i] .. term_offsets[i+1]) (term_offsets may be NULL: no
+ * energies).  tile_bits (local qubits of a work tile, 6..12 FP64, 6..13 FP32) 0 = chosen by
+ * the autotuner: the candidate tile sizes and block sizes are timed on the batch itself and
+ * the fastest kept; the choice is cached per batch shape (precision, device, qubit and gate
+ * counts) for later batches of that shape. */
+typedef struct svb_circuit_batch svb_circuit_batch;
+
+typedef struct {
+    uint32_t n_circuits;
+    uint32_t n_phases;            /* grid-wide phases of one launch */
+    uint32_t tile_bits;           /* local qubits of a work tile */
+    uint32_t threads;             /* threads per CTA */
+    uint64_t pool_amplitudes;     /* sum over circuits of 2^n */
+    uint64_t items;               /* (circuit, pass, tile) work items of one run */
+    uint32_t grid;                /* resident CTAs of the persistent launch */
+    uint32_t graphed;             /* 1 if a run replays a CUDA graph */
+    double moved_bytes;           /* state bytes one run reads and writes (passes x 2 x state) */
+    uint32_t tuned;               /* 1 if the autotuner chose tile_bits and threads */
+    uint32_t n_passes;
+} svb_cbatch_stats;
+
+svb_status svb_cbatch_create(int device, int precision, uint32_t n_circuits, const uint32_t* n_qubits,
+                             const uint64_t* gate_offsets, const svb_gate* gates,
+                             const uint64_t* term_offsets, const svb_pauli_term* terms,
+                             int tile_bits, svb_circuit_batch** out);
+
+/* Runs every circuit from |0..0> and writes energies[i] = Re <psi_i| H_i |psi_i> (0 for a
+ * circuit without terms; energies may be NULL).  `gates` NULL runs the gates given at
+ * creation; otherwise the same gate structure (ops and qubits) with new angles, e.g.
+ * another set of parameters.  Blocks until the energies are on the host. */
+svb_status svb_cbatch_run(svb_circuit_batch* batch, const svb_gate* gates, double* energies);
+
+/* The final state of one circuit of the last run, as SoA host arrays (2^n doubles each). */
+svb_status svb_cbatch_get_state(svb_circuit_batch* batch, uint32_t circuit, double* re, double* im);
+
+svb_status svb_cbatch_info(const svb_circuit_batch* batch, svb_cbatch_stats* out);
+
+svb_status svb_cbatch_destroy(svb_circuit_batch* batch);
+
 /* ---- diagnostics ---------------------------------------------------------------- */
 
 /* Message of the last failed call on this thread ("" if none). */
@@ -308,6 +383,11 @@ const char* svb_version(void);
  * tensor-core MMAs (mma.sync m8n8k4 f64, 8 independent chains per warp) on `device` for a
  * few milliseconds and writes the rate in TFLOP/s: the bound of the pair engine's blocks. */
 svb_status svb_fp64_mma_peak(int device, double* tflops);
+
+/* No reference counterpart (a measurement helper): the L2 copy bandwidth of `device` in
+ * GB/s (read + write bytes), from a copy between two 16 MiB buffers repeated inside one
+ * launch: the bound of states small enough to stay in L2. */
+svb_status svb_l2_copy_peak(int device, double* gbs);
 
 #ifdef __cplusplus
 }

@@ -19,7 +19,12 @@
 //   * upload() is one host-side validation + planning step, not O(gates) cudaMalloc /
 //     cudaMemcpy calls (:110-160);
 //   * measure() samples on the GPU with the reference's rule and its rand() draws;
-//   * the host arrays are ordinary heap memory, zero pages mapped lazily.
+//   * sv_real_cpu / sv_imag_cpu are filled lazily: sim() leaves the state on the GPU and
+//     the first read of either array after it (sv_real_cpu[i], or taking it as a
+//     ValType*) copies the whole state back once.  The reference copies 2^n x 16 bytes
+//     back after every sim() (svsim_nvgpu_sin.cuh:328-329) whether or not the caller
+//     reads them; a program that only samples never pays that copy here.  The host
+//     arrays are ordinary heap memory, zero pages mapped lazily.
 #ifndef SVSIM_NVGPU_SIN_CUH
 #define SVSIM_NVGPU_SIN_CUH
 
@@ -95,6 +100,26 @@ public:
     ValType lambda;
 };
 
+class Simulation;
+
+// One of the two host arrays of the state.  Indexing it, or converting it to ValType*,
+// first brings the host copy up to date with the device state (both arrays at once).
+class HostStateArray
+{
+public:
+    ValType& operator[](IdxType i) { sync(); return data_[i]; }
+    const ValType& operator[](IdxType i) const { sync(); return data_[i]; }
+    operator ValType*() { sync(); return data_; }
+    operator const ValType*() const { sync(); return data_; }
+
+private:
+    friend class Simulation;
+    HostStateArray() : data_(NULL), owner_(NULL) {}
+    inline void sync() const;
+    ValType* data_;
+    Simulation* owner_;
+};
+
 class Simulation
 {
 public:
@@ -102,18 +127,20 @@ public:
         : n_qubits(_n_qubits), i_gpu(_i_gpu),
           dim((IdxType)1 << _n_qubits), half_dim((IdxType)1 << (_n_qubits - 1)),
           sv_size(((IdxType)1 << _n_qubits) * (IdxType)sizeof(ValType)),
-          n_gates(0), sv_real_cpu(NULL), sv_imag_cpu(NULL), gpu_mem(0), handle(NULL)
+          n_gates(0), gpu_mem(0), handle(NULL), host_stale(false)
     {
         check(svb_create((uint32_t)n_qubits, (int)i_gpu, SVB_FP64, &handle), "Simulation");
-        sv_real_cpu = static_cast<ValType*>(std::calloc(dim, sizeof(ValType)));
-        sv_imag_cpu = static_cast<ValType*>(std::calloc(dim, sizeof(ValType)));
-        if (!sv_real_cpu || !sv_imag_cpu) {
-            std::free(sv_real_cpu);
-            std::free(sv_imag_cpu);
+        sv_real_cpu.owner_ = this;
+        sv_imag_cpu.owner_ = this;
+        sv_real_cpu.data_ = static_cast<ValType*>(std::calloc(dim, sizeof(ValType)));
+        sv_imag_cpu.data_ = static_cast<ValType*>(std::calloc(dim, sizeof(ValType)));
+        if (!sv_real_cpu.data_ || !sv_imag_cpu.data_) {
+            std::free(sv_real_cpu.data_);
+            std::free(sv_imag_cpu.data_);
             svb_destroy(handle);
             throw std::runtime_error("Simulation: host state allocation failed");
         }
-        sv_real_cpu[0] = 1.;
+        sv_real_cpu.data_[0] = 1.;
         gpu_mem = (ValType)(2 * sv_size);
     }
 
@@ -121,8 +148,17 @@ public:
     {
         clear_circuit();
         svb_destroy(handle);
-        std::free(sv_real_cpu);
-        std::free(sv_imag_cpu);
+        std::free(sv_real_cpu.data_);
+        std::free(sv_imag_cpu.data_);
+    }
+
+    // Copies the device state into sv_real_cpu / sv_imag_cpu if it changed since the
+    // last copy (called by the arrays themselves on access).
+    void sync_host_state()
+    {
+        if (!host_stale) return;
+        check(svb_get_state_soa(handle, sv_real_cpu.data_, sv_imag_cpu.data_), "sv_real_cpu");
+        host_stale = false;
     }
 
     void reset()
@@ -134,9 +170,10 @@ public:
     void reset_sv()
     {
         check(svb_reset_state(handle), "reset_sv");
-        std::memset(sv_real_cpu, 0, sv_size);
-        std::memset(sv_imag_cpu, 0, sv_size);
-        sv_real_cpu[0] = 1;
+        std::memset(sv_real_cpu.data_, 0, sv_size);
+        std::memset(sv_imag_cpu.data_, 0, sv_size);
+        sv_real_cpu.data_[0] = 1;
+        host_stale = false;
     }
 
     // The gate is copied (pybind11 owns and frees the factory's object).
@@ -166,15 +203,15 @@ public:
         return ss.str();
     }
 
-    // Runs the uploaded circuit on the device state, then copies the state back into
-    // sv_real_cpu / sv_imag_cpu as the reference does after every run.
+    // Runs the uploaded circuit on the device state.  sv_real_cpu / sv_imag_cpu follow
+    // on their next read (the reference copies them back here, :328-329).
     void sim()
     {
         const double t0 = wall_ms();
         check(svb_run(handle, NULL), "sim");
         check(svb_synchronize(handle), "sim");
         const double sim_time = wall_ms() - t0;
-        check(svb_get_state_soa(handle, sv_real_cpu, sv_imag_cpu), "sim");
+        host_stale = true;
 #ifdef PRINT_MEA_PER_CIRCUIT
         printf("\n============== SV-Sim: NVIDIA-GPU-SIN (B200) ===============\n");
         printf("nqubits:%llu, ngates:%llu, ncores:%d, sim:%.3lf ms, mem:%.3lf MB, mem_per_gpu:%.3lf MB\n",
@@ -287,11 +324,12 @@ public:
     const IdxType half_dim;
     const IdxType sv_size;
     IdxType n_gates;
-    ValType* sv_real_cpu;     // host copy of the state, refreshed by sim()
-    ValType* sv_imag_cpu;
+    HostStateArray sv_real_cpu;   // host copy of the state, filled on first read after sim()
+    HostStateArray sv_imag_cpu;
     ValType gpu_mem;          // bytes of device state, as a double (as the reference)
     vector<Gate*> circuit;
     svb_sim* handle;          // the engine behind this simulation
+    bool host_stale;          // the device state changed since the last host copy
 
 private:
     static void check(svb_status st, const char* where)
@@ -307,6 +345,11 @@ private:
     Simulation(const Simulation&);
     Simulation& operator=(const Simulation&);
 };
+
+inline void HostStateArray::sync() const
+{
+    if (owner_) owner_->sync_host_state();
+}
 
 }  // namespace SVSim
 

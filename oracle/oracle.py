@@ -18,6 +18,9 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# Where the reference tree is read from when the checkers are built (the one setting;
+# oracle/Makefile takes it as REF).
+REFERENCE = os.environ.get("SVSIM_REFERENCE", "/root/reference")
 BUILD = os.path.join(HERE, "_build")
 REF = os.path.join(HERE, "_ref")
 
@@ -32,9 +35,9 @@ def _ptr(a, t=_dp):
 def build(reference: bool = True) -> None:
     """Build the restatement, and the reference backends when the reference tree exists."""
     targets = ["oracle"]
-    if reference and os.path.isdir("/root/reference/svsim/src"):
+    if reference and os.path.isdir(os.path.join(REFERENCE, "svsim", "src")):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE}"] + targets, check=True)
 
 
 class Oracle:

@@ -10,7 +10,9 @@
 // Only psi and lambda are held; to bound the drift of the reverse-propagated psi the
 // forward pass stores checkpoints, and psi is reloaded from them on the way back.
 // Every reduction is FP64 with a fixed order (per-block partials, then one pass).
-// The forward pass runs on the staged engine; the reverse sweep is tiled: its inverse ops
+// The forward pass runs on the pair engine (n >= 12; all segments planned before the
+// first launch, so the GPU never waits for the host) or the staged engine below; the
+// reverse sweep is tiled: its inverse ops
 // are cut into passes of local qubits, and each tile of psi and lambda goes through a
 // pass's ops in shared memory, leaving one derivative sum per tile and parameter slot.
 #include <cmath>
@@ -382,6 +384,45 @@ bool inverse_op(const EOp& e, EOp& inv)
 
 using namespace svb;
 
+namespace svb {
+namespace {
+
+// Appends the pair plan of one forward segment to `all`, shifting its indices; the
+// kernel reads every index relative to its pass, so the passes of all segments can live
+// in one set of device buffers.  False if the layout indices would overflow.
+bool append_pair_plan(PairPlan& all, const PairPlan& seg)
+{
+    const int32_t op0 = (int32_t)all.ops.size(), lay0 = (int32_t)all.layouts.size();
+    const int32_t g0 = (int32_t)(all.gates.size() / 64);
+    if (all.layouts.size() + seg.layouts.size() > 65535) return false;
+    for (PairPass P : seg.passes) {
+        P.op_begin += op0;
+        P.op_end += op0;
+        P.load_layout += lay0;
+        P.store_layout += lay0;
+        P.gate_begin += g0;
+        all.passes.push_back(P);
+    }
+    for (PairOp o : seg.ops) {
+        if (o.kind == PO_BLOCK) o.gate += (uint32_t)g0;
+        else if (o.kind == PO_RELAYOUT) {
+            o.layout = (uint16_t)(o.layout + lay0);
+            o.src = (uint16_t)(o.src + lay0);
+        }
+        all.ops.push_back(o);
+    }
+    all.layouts.insert(all.layouts.end(), seg.layouts.begin(), seg.layouts.end());
+    all.gates.insert(all.gates.end(), seg.gates.begin(), seg.gates.end());
+    all.stage_bytes = std::max(all.stage_bytes, seg.stage_bytes);
+    all.n_blocks += seg.n_blocks;
+    return true;
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace svb
+
 extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_param_binding* bindings,
                                   size_t n_gates, uint32_t n_params, const svb_pauli_term* terms,
                                   size_t n_terms, double* energy, double* grad)
@@ -476,14 +517,19 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
                                      cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(err, "terms upload");
 
-    // checkpoints: up to 4 evenly spaced, if they fit in a quarter of free memory
+    // checkpoints: up to 4 evenly spaced, if they fit in a quarter of free memory (the
+    // device is asked once per state size; later calls reuse the answer)
     std::vector<void*> ckpts;
     std::vector<size_t> ckpt_at;   // op index where checkpoint c was taken (state before op)
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
-    size_t held = 0;
-    for (const GrowBuf& b : A.ckpts) held += b.cap >= sbytes ? sbytes : 0;
-    int n_ck = (int)std::min<size_t>(4, (free_b + held) / 4 / sbytes);
+    if (A.ck_count < 0 || A.ck_bytes != sbytes) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        size_t held = 0;
+        for (const GrowBuf& b : A.ckpts) held += b.cap >= sbytes ? sbytes : 0;
+        A.ck_count = (int)std::min<size_t>(4, (free_b + held) / 4 / sbytes);
+        A.ck_bytes = sbytes;
+    }
+    int n_ck = A.ck_count;
     if (K < 64) n_ck = 0;
     if ((int)A.ckpts.size() < n_ck) A.ckpts.resize(n_ck);
     for (int c = 0; c < n_ck; c++) {
@@ -492,21 +538,84 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
         ckpt_at.push_back(K * (size_t)(c + 1) / (size_t)(n_ck + 1));
     }
 
-    // forward, segment by segment
-    if ((err = launch_reset<double>(s->state, n, nullptr)) != cudaSuccess) return fail(err, "reset");
-    size_t begin = 0;
-    for (size_t c = 0; c <= ckpts.size(); c++) {
-        const size_t end = c < ckpts.size() ? ckpt_at[c] : K;
-        std::vector<EOp> seg(eops.begin() + begin, eops.begin() + end);
-        svb_status r2 = run_eops_fp64(n, s->state, seg, nullptr, A);
-        if (r2 != SVB_OK) {
-            if (!keep) free_adjoint_scratch(A);
-            return r2;
+    // the forward segments' pair plans, all built before anything is queued, so that the
+    // GPU runs the whole forward pass without waiting for the host
+    PairPlan fwd;
+    std::vector<size_t> seg_pass_end;
+    bool fwd_pairs = n >= PR_TILE_BITS;
+    {
+        size_t b0 = 0;
+        for (size_t c = 0; fwd_pairs && c <= ckpts.size(); c++) {
+            const size_t e0 = c < ckpts.size() ? ckpt_at[c] : K;
+            std::vector<EOp> seg(eops.begin() + b0, eops.begin() + e0);
+            PairPlan P;
+            if (!plan_pairs(seg, n, P) || !append_pair_plan(fwd, P)) fwd_pairs = false;
+            seg_pass_end.push_back(fwd.passes.size());
+            b0 = e0;
         }
-        if (c < ckpts.size() &&
-            (err = cudaMemcpyAsync(ckpts[c], s->state, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
-            return fail(err, "checkpoint");
-        begin = end;
+    }
+    // pinned staging: [forward plan | reverse plan | results]
+    const size_t fwd_bytes = align_up(fwd.passes.size() * sizeof(PairPass)) +
+                             align_up(fwd.ops.size() * sizeof(PairOp)) +
+                             align_up(fwd.layouts.size() * sizeof(DevStage)) +
+                             align_up(fwd.gates.size() * sizeof(double));
+    // forward, segment by segment, checkpoint copies between them
+    if ((err = launch_reset<double>(s->state, n, nullptr)) != cudaSuccess) return fail(err, "reset");
+    if (fwd_pairs && !fwd.passes.empty()) {
+        if ((err = grow_host(A.host_stage, fwd_bytes)) != cudaSuccess) return fail(err, "cudaMallocHost(stage)");
+        if ((err = grow(A.pair_passes, fwd.passes.size() * sizeof(PairPass))) != cudaSuccess ||
+            (err = grow(A.pair_ops, std::max<size_t>(1, fwd.ops.size()) * sizeof(PairOp))) != cudaSuccess ||
+            (err = grow(A.pair_layouts, std::max<size_t>(1, fwd.layouts.size()) * sizeof(DevStage))) != cudaSuccess ||
+            (err = grow(A.pair_gates, std::max<size_t>(2, fwd.gates.size()) * sizeof(double))) != cudaSuccess)
+            return fail(err, "cudaMalloc(forward plan)");
+        char* hs = static_cast<char*>(A.host_stage.p);
+        size_t off = 0;
+        auto stage = [&](const void* src, size_t bytes, void* dst) {
+            if (bytes == 0 || err != cudaSuccess) return;
+            std::memcpy(hs + off, src, bytes);
+            err = cudaMemcpyAsync(dst, hs + off, bytes, cudaMemcpyHostToDevice, nullptr);
+            off += align_up(bytes);
+        };
+        stage(fwd.passes.data(), fwd.passes.size() * sizeof(PairPass), A.pair_passes.p);
+        stage(fwd.ops.data(), fwd.ops.size() * sizeof(PairOp), A.pair_ops.p);
+        stage(fwd.layouts.data(), fwd.layouts.size() * sizeof(DevStage), A.pair_layouts.p);
+        stage(fwd.gates.data(), fwd.gates.size() * sizeof(double), A.pair_gates.p);
+        if (err != cudaSuccess) return fail(err, "forward plan upload");
+        DevPairBuffers pb;
+        pb.passes = static_cast<PairPass*>(A.pair_passes.p);
+        pb.ops = static_cast<PairOp*>(A.pair_ops.p);
+        pb.layouts = static_cast<DevStage*>(A.pair_layouts.p);
+        pb.gates = static_cast<double*>(A.pair_gates.p);
+        pb.stage_bytes = fwd.stage_bytes;
+        size_t p0 = 0;
+        for (size_t c = 0; c <= ckpts.size(); c++) {
+            for (size_t p = p0; p < seg_pass_end[c] && err == cudaSuccess; p++)
+                err = launch_pair_pass(s->state, n, (int)p, pb, nullptr);
+            if (err != cudaSuccess) return fail(err, "forward pass");
+            p0 = seg_pass_end[c];
+            if (c < ckpts.size() &&
+                (err = cudaMemcpyAsync(ckpts[c], s->state, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
+                return fail(err, "checkpoint");
+        }
+    } else if (fwd_pairs) {
+        for (void* ck : ckpts)
+            if ((err = cudaMemcpyAsync(ck, s->state, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
+                return fail(err, "checkpoint");
+    } else {
+        size_t begin = 0;
+        for (size_t c = 0; c <= ckpts.size(); c++) {
+            const size_t end = c < ckpts.size() ? ckpt_at[c] : K;
+            std::vector<EOp> seg(eops.begin() + begin, eops.begin() + end);
+            svb_status r2 = run_eops_fp64(n, s->state, seg, nullptr, A);
+            if (r2 != SVB_OK) {
+                if (!keep) free_adjoint_scratch(A);
+                return r2;
+            }
+            if (c < ckpts.size() &&
+                (err = cudaMemcpyAsync(ckpts[c], s->state, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
+                return fail(err, "checkpoint");
+            begin = end;
+        }
     }
     // psi(p), handed back in the handle at the end
     if ((err = cudaMemcpyAsync(A.final_state.p, s->state, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
@@ -623,15 +732,33 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
         return fail(err, "cudaMalloc(reverse plan)");
     if ((err = grow(A.rev_slots, std::max<size_t>(1, tslots.size()) * sizeof(int32_t))) != cudaSuccess)
         return fail(err, "cudaMalloc(reverse plan)");
-    if (!tslots.empty() && (err = cudaMemcpyAsync(A.rev_slots.p, tslots.data(), tslots.size() * sizeof(int32_t),
-                                                  cudaMemcpyHostToDevice)) != cudaSuccess)
-        return fail(err, "reverse plan upload");
-    if (!tpasses.empty() && (err = cudaMemcpyAsync(A.rev_passes.p, tpasses.data(), tpasses.size() * sizeof(AdjTilePass),
-                                                   cudaMemcpyHostToDevice)) != cudaSuccess)
-        return fail(err, "reverse plan upload");
-    if (!tops.empty() && (err = cudaMemcpyAsync(A.rev_ops.p, tops.data(), tops.size() * sizeof(AdjTileOp),
-                                                cudaMemcpyHostToDevice)) != cudaSuccess)
-        return fail(err, "reverse plan upload");
+    // the reverse plan goes through the pinned stage behind the forward plan (the forward
+    // plan's copies may still be in flight, so its part of the stage is left alone); the
+    // results come back into the stage's tail
+    const size_t rev_bytes = align_up(tslots.size() * sizeof(int32_t)) +
+                             align_up(tpasses.size() * sizeof(AdjTilePass)) +
+                             align_up(tops.size() * sizeof(AdjTileOp));
+    const size_t res_bytes = (slots.size() + 1) * sizeof(double);
+    if (A.host_stage.cap < fwd_bytes + rev_bytes + res_bytes) {
+        // growing would free memory the forward copies may still read: wait for them
+        if ((err = cudaStreamSynchronize(nullptr)) != cudaSuccess) return fail(err, "forward pass");
+        if ((err = grow_host(A.host_stage, fwd_bytes + rev_bytes + res_bytes)) != cudaSuccess)
+            return fail(err, "cudaMallocHost(stage)");
+    }
+    {
+        char* hs = static_cast<char*>(A.host_stage.p);
+        size_t off = fwd_bytes;
+        auto stage = [&](const void* src, size_t bytes, void* dst) {
+            if (bytes == 0 || err != cudaSuccess) return;
+            std::memcpy(hs + off, src, bytes);
+            err = cudaMemcpyAsync(dst, hs + off, bytes, cudaMemcpyHostToDevice, nullptr);
+            off += align_up(bytes);
+        };
+        stage(tslots.data(), tslots.size() * sizeof(int32_t), A.rev_slots.p);
+        stage(tpasses.data(), tpasses.size() * sizeof(AdjTilePass), A.rev_passes.p);
+        stage(tops.data(), tops.size() * sizeof(AdjTileOp), A.rev_ops.p);
+        if (err != cudaSuccess) return fail(err, "reverse plan upload");
+    }
     double2* psi = static_cast<double2*>(s->state);
     {
         static int ctas_per_sm = 0, sms = 0;
@@ -665,10 +792,13 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
     if (!slots.empty())
         k_reduce_rows<<<(unsigned)((slots.size() * 32 + 255) / 256), 256>>>(partial, (int)tiles, tiles,
                                                                           (int)slots.size(), results);
-    std::vector<double> host(slots.size() + 1);
-    if ((err = cudaMemcpy(host.data(), results, host.size() * sizeof(double), cudaMemcpyDeviceToHost)) !=
-        cudaSuccess)
+    // results to the stage's tail, psi(p) back into the handle, then one wait
+    double* host = reinterpret_cast<double*>(static_cast<char*>(A.host_stage.p) + fwd_bytes + rev_bytes);
+    if ((err = cudaMemcpyAsync(host, results, res_bytes, cudaMemcpyDeviceToHost, nullptr)) != cudaSuccess)
         return fail(err, "results download");
+    if ((err = cudaMemcpyAsync(s->state, A.final_state.p, sbytes, cudaMemcpyDeviceToDevice, nullptr)) != cudaSuccess)
+        return fail(err, "final state restore");
+    if ((err = cudaStreamSynchronize(nullptr)) != cudaSuccess) return fail(err, "adjoint");
     if (energy) *energy = host[slots.size()];
     for (uint32_t p = 0; p < n_params; p++) grad[p] = 0.0;
     for (size_t r = 0; r < slots.size(); r++) {
@@ -678,9 +808,6 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
             if (b.idx[f] >= 0 && e.jac[slots[r].i][f] != 0.0)
                 grad[b.idx[f]] += 2.0 * host[r] * e.jac[slots[r].i][f] * b.coef[f];
     }
-    // leave psi(p) in the handle
-    if ((err = cudaMemcpy(s->state, A.final_state.p, sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
-        return fail(err, "final state restore");
     if (!keep) free_adjoint_scratch(A);
     return SVB_OK;
 }

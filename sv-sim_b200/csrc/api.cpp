@@ -87,8 +87,7 @@ void free_plan(Sim* s)
 void free_scratch(Sim* s)
 {
     free_adjoint_scratch(s->adj);
-    cudaFree(s->mscr.block_sums);
-    cudaFree(s->mscr.block_prefix);
+    cudaFree(s->mscr.cdf);
     cudaFree(s->mscr.uniforms);
     cudaFree(s->mscr.samples);
     cudaFree(s->mscr.partial);
@@ -98,15 +97,12 @@ void free_scratch(Sim* s)
 svb_status ensure_scratch(Sim* s, size_t shots)
 {
     const size_t nb = measure_scratch_doubles((int)s->n);
-    if (s->mscr.cap_blocks < nb) {
-        cudaFree(s->mscr.block_sums);
-        cudaFree(s->mscr.block_prefix);
-        s->mscr.block_sums = s->mscr.block_prefix = nullptr;
-        s->mscr.cap_blocks = 0;
-        SVB_CUDA(cudaMalloc(&s->mscr.block_sums, nb * sizeof(double)), "cudaMalloc(block sums)");
-        SVB_CUDA(cudaMalloc(&s->mscr.block_prefix, (nb + 1) * sizeof(double)),
-                 "cudaMalloc(block prefix)");
-        s->mscr.cap_blocks = nb;
+    if (s->mscr.cap_doubles < nb) {
+        cudaFree(s->mscr.cdf);
+        s->mscr.cdf = nullptr;
+        s->mscr.cap_doubles = 0;
+        SVB_CUDA(cudaMalloc(&s->mscr.cdf, nb * sizeof(double)), "cudaMalloc(measurement workspace)");
+        s->mscr.cap_doubles = nb;
     }
     if (s->mscr.cap_shots < shots) {
         cudaFree(s->mscr.uniforms);
@@ -218,6 +214,25 @@ void release(GrowBuf& b)
     b = GrowBuf{};
 }
 
+cudaError_t grow_host(GrowBuf& b, size_t bytes)
+{
+    if (b.cap >= bytes && b.p) return cudaSuccess;
+    cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    const size_t want = std::max<size_t>(bytes, 4096);
+    const cudaError_t e = cudaMallocHost(&b.p, want);
+    if (e == cudaSuccess) b.cap = want;
+    else b.p = nullptr;
+    return e;
+}
+
+void release_host(GrowBuf& b)
+{
+    cudaFreeHost(b.p);
+    b = GrowBuf{};
+}
+
 void free_adjoint_scratch(AdjScratch& a)
 {
     release(a.lam);
@@ -235,8 +250,11 @@ void free_adjoint_scratch(AdjScratch& a)
     release(a.rev_passes);
     release(a.rev_ops);
     release(a.rev_slots);
+    release_host(a.host_stage);
     for (GrowBuf& b : a.ckpts) release(b);
     a.ckpts.clear();
+    a.ck_count = -1;
+    a.ck_bytes = 0;
 }
 
 svb_status run_eops_fp64(int n, void* state, const std::vector<EOp>& ops, cudaStream_t st, AdjScratch& cache)
@@ -602,9 +620,11 @@ svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* g
         s->info.n_passes = s->eops.size();
         s->info.tile_bits = 0;
         double moved = 0;
+        // dense forms read and write every amplitude (2 sb); diagonal forms other than
+        // DIAG and CX read and write one half of the state (its |1> half, resp. its
+        // control = 1 half: sb).  F_M4 blocks count as dense.
         for (const EOp& e : s->eops)
-            moved += (e.form == F_CX) ? 0.5 * sb : (form_is_diag(e.form) && e.form != F_DIAG) ? sb : 2.0 * sb;
-        // (F_M4 blocks count as dense: one read and one write)
+            moved += (e.form == F_CX || (form_is_diag(e.form) && e.form != F_DIAG)) ? sb : 2.0 * sb;
         s->info.moved_bytes = moved;
     }
     s->have_circuit = true;
@@ -778,8 +798,17 @@ svb_status svb_measure_seeded(svb_sim* s, uint32_t seed, uint32_t shots, uint64_
 
 svb_status svb_norm2(svb_sim* s, double* out)
 {
-    if (!out) return invalid("svb_norm2: NULL output");
-    return svb_measure(s, nullptr, 0, nullptr, out);
+    if (!s || !out) return invalid("svb_norm2: NULL argument");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    svb_status rc = ensure_scratch(s, 1);
+    if (rc != SVB_OK) return rc;
+    cudaError_t e = dispatch_prec(s->precision, [&](auto t) {
+        using T = decltype(t);
+        return norm2_device<T>(s->state, (int)s->n, s->d_small, s->mscr, nullptr);
+    });
+    if (e != cudaSuccess) return cuda_fail(e, "norm2");
+    SVB_CUDA(cudaMemcpy(out, s->d_small, sizeof(double), cudaMemcpyDeviceToHost), "norm download");
+    return SVB_OK;
 }
 
 svb_status svb_compare_states(svb_sim* a, svb_sim* b, double* fidelity, double* max_abs_diff)

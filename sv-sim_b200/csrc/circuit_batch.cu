@@ -1,0 +1,798 @@
+// Batched circuits (no counterpart in the reference): many independent circuits, each on
+// its own state of n_i qubits (any mix of sizes up to 24), run from |0..0> by one
+// persistent cooperative launch that a CUDA graph replays, with an optional Pauli-sum
+// energy per circuit.  The reference runs one circuit per Simulation and one launch per
+// sim() (svsim_nvgpu_sin.cuh:306-339) with a fixed launch shape (:309-316, config.hpp:48);
+// here the tile size and block size are chosen per batch by timing candidates (the
+// autotuner below).
+//
+// Plan.  Each circuit is lowered to the reference's elementary ops (lower.cpp).  A circuit
+// of n <= MB qubits is one tile holding its whole state: all its ops in one pass.  Larger
+// circuits are cut into passes of MB local qubits by the shared pass cut (select_passes):
+// dense and CX targets are local; a diagonal op or a CX control on a non-local qubit is
+// resolved per tile (the qubit's value is fixed across the tile).
+//
+// Launch.  Phase p processes pass p of every circuit that has one: the work items are
+// (circuit, pass, tile), spread over the resident CTAs; phases are separated by a grid
+// barrier whose wait is bounded (an error flag, then the host reports the failure).  A CTA
+// loads its tile into shared memory (gather through two offset tables per pass), applies
+// the pass's ops in order with one sweep over the tile each, and writes the tile back.
+// After the last phase, each circuit's energy sum_t c_t Re <psi| P_t |psi> is summed per
+// chunk of 4,096 amplitudes by one warp each and per circuit in a fixed order (FP64,
+// repeatable).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gate_math.cuh"
+
+namespace svb {
+namespace {
+
+constexpr unsigned kCbSpinLimit = 1u << 24;    // x >= 64 ns sleeps: > 1 s per barrier
+constexpr int CB_CHUNK = 4096;                 // amplitudes per energy chunk
+constexpr int CB_MAX_QUBITS = 24;
+
+struct CbOp {                    // 80 bytes
+    uint8_t form;
+    uint8_t p;                   // local position of the target (dense, CX) or of a local diagonal qubit
+    uint8_t c;                   // CX: local position of a local control
+    uint8_t flags;               // 1: the diagonal qubit is non-local; 2: the CX control is non-local
+    uint8_t tb;                  // the tile-index bit of that non-local qubit
+    uint8_t pad[3];
+    double m[8];
+    uint64_t pad2;
+};
+static_assert(sizeof(CbOp) == 80, "CbOp layout");
+
+struct CbPass {
+    uint64_t g_lo[64];           // local index bits 0..5 -> offset in the circuit's state
+    uint64_t g_hi[128];          // local index bits 6..12 -> offset
+    uint8_t nonlocal_q[64];      // tile-index bit j -> qubit
+    int32_t n_nonlocal, M, op_begin, op_end;
+};
+static_assert(sizeof(CbPass) % 16 == 0, "CbPass layout");
+
+struct CbCircuit {
+    uint64_t state_off;          // first amplitude of the circuit in the pool
+    uint32_t n;
+    uint32_t term_begin, term_end;
+    uint32_t chunk_begin;        // its first energy chunk
+};
+
+struct CbItem {
+    uint32_t circuit;
+    uint32_t pass;
+    uint64_t tile;
+};
+
+struct CbArgs {
+    void* pool;
+    const CbCircuit* circ;
+    const CbPass* passes;
+    const CbOp* ops;
+    const CbItem* items;
+    const uint32_t* phase_off;   // [n_phases + 1]
+    const svb_pauli_term* terms;
+    const uint32_t* chunk_circ;  // energy chunk -> circuit
+    double* partial;             // [n_chunks]
+    double* energy;              // [n_circ]
+    unsigned* barrier;           // [0] arrivals (zeroed before each launch), [1] error flag
+    int n_phases;
+    int n_circ;
+    uint32_t n_chunks;
+    int pad;
+};
+
+svb_status cb_invalid(const std::string& msg)
+{
+    set_error(msg);
+    return SVB_ERR_INVALID;
+}
+
+svb_status cb_cuda_fail(cudaError_t e, const char* what)
+{
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    (void)cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? SVB_ERR_OOM : SVB_ERR_CUDA;
+}
+
+__device__ __forceinline__ unsigned cb_ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier with a bounded wait (the launch is cooperative, so every block is
+// resident and the wait ends; past the limit the error flag is raised and the block goes on).
+__device__ __forceinline__ void cb_grid_barrier(unsigned* bar, unsigned target)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        unsigned spins = 0;
+        while (cb_ld_acquire(bar) < target) {
+            if (++spins > kCbSpinLimit || cb_ld_acquire(bar + 1) != 0u) {
+                atomicOr(bar + 1, 1u);
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t insert_zero32(uint32_t x, int b)
+{
+    return ((x >> b) << (b + 1)) | (x & ((1u << b) - 1u));
+}
+
+template <typename T>
+__device__ void cb_apply(typename VecOf<T>::type* tile, int M, const CbOp& op, uint64_t tile_index)
+{
+    const Coef<T> c = load_coef<T>(op.m);
+    const uint32_t half = 1u << (M - 1);
+    const uint32_t pd = 1u << op.p;
+    if (op.form == F_CX) {
+        if ((op.flags & 2) && !((tile_index >> op.tb) & 1ull)) return;
+        for (uint32_t t = threadIdx.x; t < half; t += blockDim.x) {
+            const uint32_t l0 = insert_zero32(t, op.p);
+            if (!(op.flags & 2) && !((l0 >> op.c) & 1u)) continue;
+            const auto a = tile[l0];
+            tile[l0] = tile[l0 | pd];
+            tile[l0 | pd] = a;
+        }
+    } else if (form_is_diag(op.form)) {
+        if (op.flags & 1) {              // the qubit is fixed across the tile
+            const bool one = (tile_index >> op.tb) & 1ull;
+            if (!one && op.form != F_DIAG) return;
+            for (uint32_t l = threadIdx.x; l < 2 * half; l += blockDim.x) {
+                if (one) diag_one<T>(op.form, c, tile[l]);
+                else diag_zero<T>(op.form, c, tile[l]);
+            }
+        } else {
+            for (uint32_t t = threadIdx.x; t < half; t += blockDim.x) {
+                const uint32_t l0 = insert_zero32(t, op.p);
+                diag_one<T>(op.form, c, tile[l0 | pd]);
+                if (op.form == F_DIAG) diag_zero<T>(op.form, c, tile[l0]);
+            }
+        }
+    } else {
+        for (uint32_t t = threadIdx.x; t < half; t += blockDim.x) {
+            const uint32_t l0 = insert_zero32(t, op.p);
+            dense_pair<T>(op.form, c, tile[l0], tile[l0 | pd]);
+        }
+    }
+}
+
+__device__ __forceinline__ double cb_warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_cbatch(CbArgs A)
+{
+    using V = typename VecOf<T>::type;
+    extern __shared__ __align__(16) unsigned char cb_smem[];
+    CbPass* sp = reinterpret_cast<CbPass*>(cb_smem);
+    V* tile = reinterpret_cast<V*>(cb_smem + sizeof(CbPass));
+    __shared__ int cur_pass;
+    V* pool = static_cast<V*>(A.pool);
+    if (threadIdx.x == 0) cur_pass = -1;
+    __syncthreads();
+    unsigned target = 0;
+    for (int ph = 0; ph < A.n_phases; ph++) {
+        for (uint32_t it = A.phase_off[ph] + blockIdx.x; it < A.phase_off[ph + 1]; it += gridDim.x) {
+            const CbItem item = A.items[it];
+            if ((int)item.pass != cur_pass) {
+                const uint4* src = reinterpret_cast<const uint4*>(A.passes + item.pass);
+                uint4* dst = reinterpret_cast<uint4*>(sp);
+                for (int w = threadIdx.x; w < (int)(sizeof(CbPass) / 16); w += blockDim.x) dst[w] = src[w];
+                __syncthreads();
+                if (threadIdx.x == 0) cur_pass = (int)item.pass;
+            }
+            const CbCircuit C = A.circ[item.circuit];
+            const int M = sp->M;
+            const uint32_t TL = 1u << M;
+            uint64_t base = C.state_off;
+            for (int j = 0; j < sp->n_nonlocal; j++) base |= ((item.tile >> j) & 1ull) << sp->nonlocal_q[j];
+            for (uint32_t l = threadIdx.x; l < TL; l += blockDim.x) tile[l] = pool[base + sp->g_lo[l & 63u] + sp->g_hi[l >> 6]];
+            __syncthreads();
+            for (int o = sp->op_begin; o < sp->op_end; o++) {
+                const CbOp op = A.ops[o];
+                cb_apply<T>(tile, M, op, item.tile);
+                __syncthreads();
+            }
+            for (uint32_t l = threadIdx.x; l < TL; l += blockDim.x) pool[base + sp->g_lo[l & 63u] + sp->g_hi[l >> 6]] = tile[l];
+            __syncthreads();
+        }
+        target += gridDim.x;
+        cb_grid_barrier(A.barrier, target);
+    }
+    if (A.n_chunks == 0) return;
+    // energies: one warp per chunk, then one warp per circuit over its chunks in order
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    for (uint32_t k = wid; k < A.n_chunks; k += warps) {
+        const CbCircuit C = A.circ[A.chunk_circ[k]];
+        const uint64_t dim = 1ull << C.n;
+        const uint64_t start = (uint64_t)(k - C.chunk_begin) * CB_CHUNK;
+        const uint64_t end = start + CB_CHUNK < dim ? start + CB_CHUNK : dim;
+        const V* sv = pool + C.state_off;
+        double acc = 0.0;
+        for (uint64_t i = start + lane; i < end; i += 32) {
+            const V a = sv[i];
+            const double ar = (double)a.x, ai = (double)a.y;
+            for (uint32_t t = C.term_begin; t < C.term_end; t++) {
+                const svb_pauli_term P = A.terms[t];
+                const uint64_t j = i ^ P.x_mask;
+                const V b = sv[j];
+                double br = (double)b.x, bi = (double)b.y;
+                if (__popcll(j & P.z_mask) & 1) { br = -br; bi = -bi; }
+                double tr, ti;
+                switch (__popcll(P.x_mask & P.z_mask) & 3) {     // i^(number of Y factors)
+                case 0: tr = br; ti = bi; break;
+                case 1: tr = -bi; ti = br; break;
+                case 2: tr = -br; ti = -bi; break;
+                default: tr = bi; ti = -br; break;
+                }
+                acc += P.coef * (ar * tr + ai * ti);
+            }
+        }
+        acc = cb_warp_sum(acc);
+        if (lane == 0) A.partial[k] = acc;
+    }
+    target += gridDim.x;
+    cb_grid_barrier(A.barrier, target);
+    for (uint32_t c = wid; c < (uint32_t)A.n_circ; c += warps) {
+        const CbCircuit C = A.circ[c];
+        if (C.term_end == C.term_begin) {
+            if (lane == 0) A.energy[c] = 0.0;
+            continue;
+        }
+        const uint64_t nch = ((1ull << C.n) + CB_CHUNK - 1) / CB_CHUNK;
+        double s = 0.0;
+        for (uint64_t k = lane; k < nch; k += 32) s += A.partial[C.chunk_begin + k];
+        s = cb_warp_sum(s);
+        if (lane == 0) A.energy[c] = s;
+    }
+}
+
+template <typename T>
+__global__ void k_cb_ones(void* pool, const CbCircuit* circ, int n_circ)
+{
+    using V = typename VecOf<T>::type;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_circ; c += gridDim.x * blockDim.x) {
+        V one;
+        one.x = 1;
+        one.y = 0;
+        static_cast<V*>(pool)[circ[c].state_off] = one;
+    }
+}
+
+// ---- host side ----------------------------------------------------------------------
+
+struct CbPlan {
+    std::vector<CbCircuit> circ;
+    std::vector<CbPass> passes;
+    std::vector<CbOp> ops;
+    std::vector<CbItem> items;
+    std::vector<uint32_t> phase_off;
+    std::vector<uint32_t> chunk_circ;
+    uint64_t pool_amps = 0;
+    double moved_bytes = 0;
+};
+
+CbPass make_pass(uint64_t L, int n)
+{
+    CbPass P;
+    std::memset(&P, 0, sizeof(P));
+    int local_q[64], nl = 0, nn = 0;
+    for (int q = 0; q < n; q++) {
+        if ((L >> q) & 1ull) local_q[nl++] = q;
+        else P.nonlocal_q[nn++] = (uint8_t)q;
+    }
+    P.n_nonlocal = nn;
+    P.M = nl;
+    for (int j = 0; j < 64; j++)
+        for (int b = 0; b < 6 && b < nl; b++)
+            if ((j >> b) & 1) P.g_lo[j] |= 1ull << local_q[b];
+    for (int j = 0; j < 128; j++)
+        for (int b = 0; b < 7 && 6 + b < nl; b++)
+            if ((j >> b) & 1) P.g_hi[j] |= 1ull << local_q[6 + b];
+    return P;
+}
+
+// Appends circuit ops `taken` (indices into eops) as one pass over local mask L.
+void emit_pass(CbPlan& plan, const std::vector<EOp>& eops, const std::vector<int>& taken, uint64_t L, int n)
+{
+    CbPass P = make_pass(L, n);
+    int pos[64], tbit[64];
+    for (int q = 0; q < 64; q++) pos[q] = tbit[q] = -1;
+    int nl = 0;
+    for (int q = 0; q < n; q++)
+        if ((L >> q) & 1ull) pos[q] = nl++;
+    for (int j = 0; j < P.n_nonlocal; j++) tbit[P.nonlocal_q[j]] = j;
+    P.op_begin = (int32_t)plan.ops.size();
+    for (int i : taken) {
+        const EOp& e = eops[i];
+        CbOp o;
+        std::memset(&o, 0, sizeof(o));
+        o.form = e.form;
+        std::memcpy(o.m, e.m, sizeof(o.m));
+        if (e.form == F_CX) {
+            o.p = (uint8_t)pos[e.q];
+            if (pos[e.c] >= 0) o.c = (uint8_t)pos[e.c];
+            else { o.flags |= 2; o.tb = (uint8_t)tbit[e.c]; }
+        } else if (form_is_diag(e.form)) {
+            if (pos[e.q] >= 0) o.p = (uint8_t)pos[e.q];
+            else { o.flags |= 1; o.tb = (uint8_t)tbit[e.q]; }
+        } else {
+            o.p = (uint8_t)pos[e.q];
+        }
+        plan.ops.push_back(o);
+    }
+    P.op_end = (int32_t)plan.ops.size();
+    plan.passes.push_back(P);
+}
+
+}  // namespace
+}  // namespace svb
+
+struct svb_circuit_batch {
+    int device = 0;
+    int precision = SVB_FP64;
+    uint32_t n_circ = 0;
+    int tile_bits = 12;
+    int threads = 512;
+    bool tuned = false;
+    std::vector<uint32_t> n;
+    std::vector<uint64_t> gate_off;
+    std::vector<svb_gate> gates;
+    std::vector<uint64_t> term_off;
+    std::vector<svb_pauli_term> terms;
+    svb::CbPlan plan;
+    // device
+    void* pool = nullptr;
+    svb::CbCircuit* d_circ = nullptr;
+    svb::CbPass* d_passes = nullptr;
+    svb::CbOp* d_ops = nullptr;
+    svb::CbItem* d_items = nullptr;
+    uint32_t* d_phase_off = nullptr;
+    svb_pauli_term* d_terms = nullptr;
+    uint32_t* d_chunk_circ = nullptr;
+    double* d_partial = nullptr;
+    double* d_energy = nullptr;
+    unsigned* d_bar = nullptr;
+    // pinned host
+    svb::CbOp* h_ops = nullptr;
+    double* h_energy = nullptr;
+    unsigned* h_err = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool graphed = false;
+    unsigned grid = 0;
+    size_t smem = 0;
+};
+
+namespace svb {
+namespace {
+
+void cb_free(svb_circuit_batch* b)
+{
+    if (!b) return;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    cudaFree(b->pool);
+    cudaFree(b->d_circ);
+    cudaFree(b->d_passes);
+    cudaFree(b->d_ops);
+    cudaFree(b->d_items);
+    cudaFree(b->d_phase_off);
+    cudaFree(b->d_terms);
+    cudaFree(b->d_chunk_circ);
+    cudaFree(b->d_partial);
+    cudaFree(b->d_energy);
+    cudaFree(b->d_bar);
+    cudaFreeHost(b->h_ops);
+    cudaFreeHost(b->h_energy);
+    cudaFreeHost(b->h_err);
+    delete b;
+}
+
+// The plan for tile size MB; false (with a message) on an invalid gate.
+bool cb_build_plan(const svb_circuit_batch* b, const svb_gate* gates, int MB, CbPlan& plan, std::string& err)
+{
+    plan = CbPlan{};
+    const size_t amp = b->precision == SVB_FP64 ? 16 : 8;
+    std::vector<std::vector<uint32_t>> per_phase;     // item indices per phase, built below
+    std::vector<std::vector<CbItem>> phase_items;
+    uint32_t chunks = 0;
+    for (uint32_t c = 0; c < b->n_circ; c++) {
+        const int n = (int)b->n[c];
+        CbCircuit C;
+        C.state_off = plan.pool_amps;
+        C.n = (uint32_t)n;
+        C.term_begin = (uint32_t)b->term_off[c];
+        C.term_end = (uint32_t)b->term_off[c + 1];
+        C.chunk_begin = chunks;
+        if (C.term_end > C.term_begin) {
+            const uint64_t nch = ((1ull << n) + CB_CHUNK - 1) / CB_CHUNK;
+            for (uint64_t k = 0; k < nch; k++) plan.chunk_circ.push_back(c);
+            chunks += (uint32_t)nch;
+        }
+        plan.pool_amps += 1ull << n;
+        plan.circ.push_back(C);
+        std::vector<EOp> eops;
+        for (uint64_t g = b->gate_off[c]; g < b->gate_off[c + 1]; g++) {
+            const svb_gate& gg = gates[g];
+            const int slots = gate_qubit_slots(gg.op);
+            if (slots == 0) { err = "gate " + std::to_string(g) + ": unknown op"; return false; }
+            for (int k = 0; k < slots; k++) {
+                if (gg.qb[k] >= (uint32_t)n) {
+                    err = "circuit " + std::to_string(c) + ", gate " + std::to_string(g) + ": qubit >= n";
+                    return false;
+                }
+                for (int j = 0; j < k; j++)
+                    if (gg.qb[j] == gg.qb[k]) { err = "gate " + std::to_string(g) + " repeats a qubit"; return false; }
+            }
+            lower_gate(gg, (int32_t)g, eops);
+        }
+        const int M = std::min(n, MB);
+        std::vector<uint32_t> my_passes;
+        if (n <= MB) {
+            std::vector<int> all(eops.size());
+            for (size_t i = 0; i < eops.size(); i++) all[i] = (int)i;
+            my_passes.push_back((uint32_t)plan.passes.size());
+            emit_pass(plan, eops, all, n >= 64 ? ~0ull : ((1ull << n) - 1), n);
+        } else {
+            select_passes(eops, n, M, std::min(3, M), [&](uint64_t L, const std::vector<int>& taken) {
+                my_passes.push_back((uint32_t)plan.passes.size());
+                emit_pass(plan, eops, taken, L, n);
+                return std::vector<int>{};
+            });
+        }
+        const uint64_t tiles = 1ull << (n - M);
+        for (size_t p = 0; p < my_passes.size(); p++) {
+            if (phase_items.size() <= p) phase_items.resize(p + 1);
+            for (uint64_t t = 0; t < tiles; t++) phase_items[p].push_back(CbItem{c, my_passes[p], t});
+            plan.moved_bytes += 2.0 * amp * (double)(1ull << n);
+        }
+    }
+    plan.phase_off.push_back(0);
+    for (auto& v : phase_items) {
+        plan.items.insert(plan.items.end(), v.begin(), v.end());
+        plan.phase_off.push_back((uint32_t)plan.items.size());
+    }
+    return true;
+}
+
+template <typename T>
+cudaError_t cb_launch(svb_circuit_batch* b, cudaStream_t s)
+{
+    CbArgs a;
+    a.pool = b->pool;
+    a.circ = b->d_circ;
+    a.passes = b->d_passes;
+    a.ops = b->d_ops;
+    a.items = b->d_items;
+    a.phase_off = b->d_phase_off;
+    a.terms = b->d_terms;
+    a.chunk_circ = b->d_chunk_circ;
+    a.partial = b->d_partial;
+    a.energy = b->d_energy;
+    a.barrier = b->d_bar;
+    a.n_phases = (int)b->plan.phase_off.size() - 1;
+    a.n_circ = (int)b->n_circ;
+    a.n_chunks = (uint32_t)b->plan.chunk_circ.size();
+    a.pad = 0;
+    void* args[] = {&a};
+    return cudaLaunchCooperativeKernel((const void*)k_cbatch<T>, dim3(b->grid), dim3(b->threads), args, b->smem, s);
+}
+
+// one evaluation: angles in, reset, launch, energies and the error flag out
+cudaError_t cb_enqueue(svb_circuit_batch* b, cudaStream_t s)
+{
+    const size_t amp = b->precision == SVB_FP64 ? 16 : 8;
+    cudaError_t e = cudaMemcpyAsync(b->d_ops, b->h_ops, b->plan.ops.size() * sizeof(CbOp), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->pool, 0, b->plan.pool_amps * amp, s);
+    if (e == cudaSuccess) {
+        const unsigned g = (unsigned)std::min<uint64_t>((b->n_circ + 255) / 256, 1024);
+        if (b->precision == SVB_FP64) k_cb_ones<double><<<g, 256, 0, s>>>(b->pool, b->d_circ, (int)b->n_circ);
+        else k_cb_ones<float><<<g, 256, 0, s>>>(b->pool, b->d_circ, (int)b->n_circ);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = b->precision == SVB_FP64 ? cb_launch<double>(b, s) : cb_launch<float>(b, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_energy, b->d_energy, b->n_circ * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_err, b->d_bar + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    return e;
+}
+
+template <typename Tp>
+cudaError_t upload(Tp** dst, const std::vector<Tp>& v)
+{
+    cudaError_t e = cudaMalloc(dst, std::max<size_t>(1, v.size()) * sizeof(Tp));
+    if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), v.size() * sizeof(Tp), cudaMemcpyHostToDevice);
+    return e;
+}
+
+// Builds a batch with tile size MB and block size `threads` (device buffers, graph).
+svb_status cb_create_with(svb_circuit_batch* proto, int MB, int threads, svb_circuit_batch** out)
+{
+    svb_circuit_batch* b = new svb_circuit_batch(*proto);
+    b->tile_bits = MB;
+    b->threads = threads;
+    auto fail = [&](const std::string& what, cudaError_t e) {
+        set_error("svb_cbatch_create: " + what + (e != cudaSuccess ? std::string(": ") + cudaGetErrorString(e) : ""));
+        (void)cudaGetLastError();
+        cb_free(b);
+        return e == cudaErrorMemoryAllocation ? SVB_ERR_OOM : (e == cudaSuccess ? SVB_ERR_INVALID : SVB_ERR_CUDA);
+    };
+    std::string err;
+    if (!cb_build_plan(b, b->gates.data(), MB, b->plan, err)) return fail(err, cudaSuccess);
+    const size_t amp = b->precision == SVB_FP64 ? 16 : 8;
+    cudaError_t e = cudaMalloc(&b->pool, std::max<uint64_t>(1, b->plan.pool_amps) * amp);
+    if (e == cudaSuccess) e = upload(&b->d_circ, b->plan.circ);
+    if (e == cudaSuccess) e = upload(&b->d_passes, b->plan.passes);
+    if (e == cudaSuccess) e = upload(&b->d_ops, b->plan.ops);
+    if (e == cudaSuccess) e = upload(&b->d_items, b->plan.items);
+    if (e == cudaSuccess) e = upload(&b->d_phase_off, b->plan.phase_off);
+    if (e == cudaSuccess) e = upload(&b->d_terms, b->terms);
+    if (e == cudaSuccess) e = upload(&b->d_chunk_circ, b->plan.chunk_circ);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_partial, std::max<size_t>(1, b->plan.chunk_circ.size()) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_energy, std::max<size_t>(1, b->n_circ) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_bar, 2 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_ops, std::max<size_t>(1, b->plan.ops.size()) * sizeof(CbOp));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_energy, std::max<size_t>(1, b->n_circ) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_err, sizeof(unsigned));
+    if (e != cudaSuccess) return fail("allocation", e);
+    if (!b->plan.ops.empty()) std::memcpy(b->h_ops, b->plan.ops.data(), b->plan.ops.size() * sizeof(CbOp));
+    b->smem = sizeof(CbPass) + (amp << MB);
+    const void* fn = b->precision == SVB_FP64 ? (const void*)k_cbatch<double> : (const void*)k_cbatch<float>;
+    int per_sm = 0, sms = 0;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, b->smem);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (e != cudaSuccess || per_sm < 1) return fail("kernel setup", e);
+    const uint64_t most = b->plan.items.empty() ? 1 : [&] {
+        uint64_t m = 1;
+        for (size_t p = 0; p + 1 < b->plan.phase_off.size(); p++)
+            m = std::max<uint64_t>(m, b->plan.phase_off[p + 1] - b->plan.phase_off[p]);
+        return m;
+    }();
+    b->grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * sms, std::max<uint64_t>(most, (uint64_t)sms));
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", e);
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const cudaError_t le = cb_enqueue(b, b->stream);
+        const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+        if (le == cudaSuccess && ce == cudaSuccess && g && cudaGraphInstantiate(&b->graph, g, 0) == cudaSuccess)
+            b->graphed = true;
+        else
+            b->graph = nullptr;
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+    }
+    *out = b;
+    return SVB_OK;
+}
+
+svb_status cb_run(svb_circuit_batch* b)
+{
+    *b->h_err = 0;
+    cudaError_t e = b->graphed ? cudaGraphLaunch(b->graph, b->stream) : cb_enqueue(b, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return cb_cuda_fail(e, "svb_cbatch_run");
+    if (*b->h_err) {
+        set_error("svb_cbatch_run: a grid barrier timed out; results are invalid");
+        return SVB_ERR_STATE;
+    }
+    return SVB_OK;
+}
+
+// Autotuner cache: batch signature -> (tile bits, threads).
+std::mutex g_tune_mutex;
+std::map<std::vector<uint64_t>, std::pair<int, int>> g_tune_cache;
+
+std::vector<uint64_t> signature(const svb_circuit_batch* b)
+{
+    std::vector<uint64_t> sig = {(uint64_t)b->precision, (uint64_t)b->device};
+    for (uint32_t c = 0; c < b->n_circ; c++)
+        sig.push_back(((uint64_t)b->n[c] << 40) | (b->gate_off[c + 1] - b->gate_off[c]));
+    return sig;
+}
+
+}  // namespace
+}  // namespace svb
+
+using namespace svb;
+
+extern "C" {
+
+svb_status svb_cbatch_create(int device, int precision, uint32_t n_circuits, const uint32_t* n_qubits,
+                             const uint64_t* gate_offsets, const svb_gate* gates, const uint64_t* term_offsets,
+                             const svb_pauli_term* terms, int tile_bits, svb_circuit_batch** out)
+{
+    if (!out || !n_qubits || !gate_offsets || (gate_offsets[n_circuits] && !gates)) {
+        set_error("svb_cbatch_create: NULL argument");
+        return SVB_ERR_INVALID;
+    }
+    *out = nullptr;
+    if (precision != SVB_FP64 && precision != SVB_FP32) return cb_invalid("svb_cbatch_create: bad precision");
+    if (n_circuits == 0) return cb_invalid("svb_cbatch_create: no circuits");
+    const int max_tb = precision == SVB_FP64 ? 12 : 13;
+    if (tile_bits != 0 && (tile_bits < 6 || tile_bits > max_tb))
+        return cb_invalid("svb_cbatch_create: tile_bits must be 0 (tune) or in [6, " + std::to_string(max_tb) + "]");
+    svb_circuit_batch proto;
+    proto.device = device;
+    proto.precision = precision;
+    proto.n_circ = n_circuits;
+    uint32_t max_n = 0;
+    for (uint32_t c = 0; c < n_circuits; c++) {
+        if (n_qubits[c] < 1 || n_qubits[c] > CB_MAX_QUBITS)
+            return cb_invalid("svb_cbatch_create: circuit " + std::to_string(c) + " needs 1..24 qubits");
+        if (gate_offsets[c + 1] < gate_offsets[c]) return cb_invalid("svb_cbatch_create: gate_offsets decrease");
+        max_n = std::max(max_n, n_qubits[c]);
+        proto.n.push_back(n_qubits[c]);
+    }
+    if (gate_offsets[0] != 0) return cb_invalid("svb_cbatch_create: gate_offsets[0] must be 0");
+    proto.gate_off.assign(gate_offsets, gate_offsets + n_circuits + 1);
+    proto.gates.assign(gates, gates + gate_offsets[n_circuits]);
+    if (term_offsets) {
+        if (term_offsets[0] != 0) return cb_invalid("svb_cbatch_create: term_offsets[0] must be 0");
+        if (term_offsets[n_circuits] && !terms) return cb_invalid("svb_cbatch_create: NULL terms");
+        proto.term_off.assign(term_offsets, term_offsets + n_circuits + 1);
+        proto.terms.assign(terms, terms + term_offsets[n_circuits]);
+        for (uint32_t c = 0; c < n_circuits; c++) {
+            if (term_offsets[c + 1] < term_offsets[c]) return cb_invalid("svb_cbatch_create: term_offsets decrease");
+            for (uint64_t t = term_offsets[c]; t < term_offsets[c + 1]; t++)
+                if ((terms[t].x_mask | terms[t].z_mask) >> n_qubits[c])
+                    return cb_invalid("svb_cbatch_create: a term of circuit " + std::to_string(c) + " acts on a qubit >= n");
+        }
+    } else {
+        proto.term_off.assign(n_circuits + 1, 0);
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cb_cuda_fail(e, "svb_cbatch_create");
+    if (tile_bits != 0) return cb_create_with(&proto, tile_bits, 512, out);
+
+    // autotune: the cached choice for this signature, else time the candidates
+    const std::vector<uint64_t> sig = signature(&proto);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(sig);
+        if (it != g_tune_cache.end()) {
+            svb_status st = cb_create_with(&proto, it->second.first, it->second.second, out);
+            if (st == SVB_OK) (*out)->tuned = true;
+            return st;
+        }
+    }
+    svb_circuit_batch* best = nullptr;
+    double best_ms = 0;
+    for (int tb = max_tb - 2; tb <= max_tb; tb++) {
+        for (int threads : {256, 512}) {
+            svb_circuit_batch* cand = nullptr;
+            if (cb_create_with(&proto, tb, threads, &cand) != SVB_OK) continue;
+            double ms = 1e300;
+            bool ok = cb_run(cand) == SVB_OK;           // warm-up
+            for (int r = 0; ok && r < 3; r++) {
+                const auto t0 = std::chrono::steady_clock::now();
+                ok = cb_run(cand) == SVB_OK;
+                const auto t1 = std::chrono::steady_clock::now();
+                ms = std::min(ms, std::chrono::duration<double, std::milli>(t1 - t0).count());
+            }
+            if (ok && (!best || ms < best_ms)) {
+                if (best) cb_free(best);
+                best = cand;
+                best_ms = ms;
+            } else {
+                cb_free(cand);
+            }
+        }
+    }
+    if (!best) {
+        set_error("svb_cbatch_create: no candidate configuration ran");
+        return SVB_ERR_CUDA;
+    }
+    best->tuned = true;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune_cache[sig] = {best->tile_bits, best->threads};
+    }
+    *out = best;
+    return SVB_OK;
+}
+
+svb_status svb_cbatch_run(svb_circuit_batch* b, const svb_gate* gates, double* energies)
+{
+    if (!b) return cb_invalid("svb_cbatch_run: NULL batch");
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e != cudaSuccess) return cb_cuda_fail(e, "svb_cbatch_run");
+    if (gates) {
+        // new angles for the same gate structure: re-plan and check that nothing moved
+        for (uint64_t g = 0; g < b->gate_off[b->n_circ]; g++)
+            if (gates[g].op != b->gates[g].op || std::memcmp(gates[g].qb, b->gates[g].qb, sizeof(gates[g].qb)) != 0)
+                return cb_invalid("svb_cbatch_run: gate " + std::to_string(g) + " differs from the batch's structure");
+        CbPlan plan;
+        std::string err;
+        if (!cb_build_plan(b, gates, b->tile_bits, plan, err)) return cb_invalid("svb_cbatch_run: " + err);
+        if (plan.ops.size() != b->plan.ops.size()) return cb_invalid("svb_cbatch_run: the plan's structure changed");
+        for (size_t i = 0; i < plan.ops.size(); i++)
+            if (plan.ops[i].form != b->plan.ops[i].form || plan.ops[i].p != b->plan.ops[i].p ||
+                plan.ops[i].flags != b->plan.ops[i].flags)
+                return cb_invalid("svb_cbatch_run: the plan's structure changed");
+        std::memcpy(b->h_ops, plan.ops.data(), plan.ops.size() * sizeof(CbOp));
+        std::copy(gates, gates + b->gate_off[b->n_circ], b->gates.begin());
+    }
+    svb_status st = cb_run(b);
+    if (st != SVB_OK) return st;
+    if (energies) std::memcpy(energies, b->h_energy, b->n_circ * sizeof(double));
+    return SVB_OK;
+}
+
+svb_status svb_cbatch_get_state(svb_circuit_batch* b, uint32_t circuit, double* re, double* im)
+{
+    if (!b || circuit >= b->n_circ) return cb_invalid("svb_cbatch_get_state: bad batch or circuit");
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e != cudaSuccess) return cb_cuda_fail(e, "svb_cbatch_get_state");
+    const uint64_t dim = 1ull << b->n[circuit];
+    const size_t amp = b->precision == SVB_FP64 ? 16 : 8;
+    std::vector<char> host(dim * amp);
+    e = cudaMemcpy(host.data(), static_cast<char*>(b->pool) + b->plan.circ[circuit].state_off * amp, dim * amp,
+                   cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cb_cuda_fail(e, "svb_cbatch_get_state");
+    for (uint64_t i = 0; i < dim; i++) {
+        double r, m;
+        if (b->precision == SVB_FP64) {
+            r = reinterpret_cast<const double*>(host.data())[2 * i];
+            m = reinterpret_cast<const double*>(host.data())[2 * i + 1];
+        } else {
+            r = reinterpret_cast<const float*>(host.data())[2 * i];
+            m = reinterpret_cast<const float*>(host.data())[2 * i + 1];
+        }
+        if (re) re[i] = r;
+        if (im) im[i] = m;
+    }
+    return SVB_OK;
+}
+
+svb_status svb_cbatch_info(const svb_circuit_batch* b, svb_cbatch_stats* out)
+{
+    if (!b || !out) return cb_invalid("svb_cbatch_info: NULL argument");
+    out->n_circuits = b->n_circ;
+    out->n_phases = (uint32_t)b->plan.phase_off.size() - 1;
+    out->tile_bits = (uint32_t)b->tile_bits;
+    out->threads = (uint32_t)b->threads;
+    out->pool_amplitudes = b->plan.pool_amps;
+    out->items = b->plan.items.size();
+    out->grid = b->grid;
+    out->graphed = b->graphed ? 1u : 0u;
+    out->moved_bytes = b->plan.moved_bytes;
+    out->tuned = b->tuned ? 1u : 0u;
+    out->n_passes = (uint32_t)b->plan.passes.size();
+    return SVB_OK;
+}
+
+svb_status svb_cbatch_destroy(svb_circuit_batch* b)
+{
+    if (!b) return SVB_OK;
+    cudaSetDevice(b->device);
+    cb_free(b);
+    return SVB_OK;
+}
+
+}  // extern "C"

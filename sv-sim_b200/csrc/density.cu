@@ -143,9 +143,36 @@ svb_status svb_dm_create(uint32_t n_qubits, int device, svb_sim** out)
 svb_status svb_dm_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates, const double* noise_kraus,
                               uint32_t n_kraus)
 {
-    if (!s || (n_gates && !gates) || (n_kraus && !noise_kraus)) {
+    return svb_dm_set_circuit_superops(s, gates, n_gates, noise_kraus, n_kraus, nullptr, 0);
+}
+
+svb_status svb_dm_set_circuit_superops(svb_sim* s, const svb_gate* gates, size_t n_gates,
+                                       const double* noise_kraus, uint32_t n_kraus,
+                                       const svb_superop* superops, size_t n_superops)
+{
+    if (!s || (n_gates && !gates) || (n_kraus && !noise_kraus) || (n_superops && !superops)) {
         set_error("svb_dm_set_circuit: NULL argument");
         return SVB_ERR_INVALID;
+    }
+    // per-op superoperator tables: the reference's order (r = 2 i + j for rho[i][j] on the
+    // gate's qubit) permuted into the F_M4 order of the pair (q, q + n) (a = i + 2 j)
+    std::vector<int> table_of(64, -1);
+    std::vector<Mat4> tables;
+    for (size_t t = 0; t < n_superops; t++) {
+        const uint32_t op = superops[t].op;
+        if (op >= 64 || gate_qubit_slots(op) != 1) {
+            set_error("svb_dm_set_circuit: superoperator " + std::to_string(t) + " is not for a one-qubit op");
+            return SVB_ERR_INVALID;
+        }
+        static const int sigma[4] = {0, 2, 1, 3};
+        Mat4 m;
+        for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) {
+                m[(a * 4 + b) * 2] = superops[t].m[(sigma[a] * 4 + sigma[b]) * 2];
+                m[(a * 4 + b) * 2 + 1] = superops[t].m[(sigma[a] * 4 + sigma[b]) * 2 + 1];
+            }
+        table_of[op] = (int)tables.size();
+        tables.push_back(m);
     }
     if (!s->dm_qubits) { set_error("svb_dm_set_circuit: not a density-matrix handle (svb_dm_create)"); return SVB_ERR_STATE; }
     if (n_kraus > 16) { set_error("svb_dm_set_circuit: at most 16 Kraus operators"); return SVB_ERR_INVALID; }
@@ -166,6 +193,17 @@ svb_status svb_dm_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates,
                     set_error("svb_dm_set_circuit: gate " + std::to_string(i) + " repeats a qubit");
                     return SVB_ERR_INVALID;
                 }
+        }
+        if (g.op < 64 && table_of[g.op] >= 0) {
+            // the gate's own superoperator (noise included, as the reference's noisy gates)
+            EOp b;
+            b.form = F_M4;
+            b.q = g.qb[0];
+            b.c = g.qb[0] + n;
+            b.mat = -2 - table_of[g.op];          // resolved below
+            b.gate = (int32_t)i;
+            eops.push_back(b);
+            continue;
         }
         const size_t first = eops.size();
         if (!lower_gate(g, (int32_t)i, eops)) {
@@ -195,7 +233,15 @@ svb_status svb_dm_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates,
         noise_mat = (int)mats.size();
         mats.push_back(superop(kraus.data(), (int)n_kraus));
     }
+    const int table_base = (int)mats.size();
+    mats.insert(mats.end(), tables.begin(), tables.end());
     for (const EOp& e : eops) {
+        if (e.form == F_M4 && e.mat <= -2) {
+            EOp b = e;
+            b.mat = table_base + (-2 - e.mat);
+            dm.push_back(b);
+            continue;
+        }
         if (e.form == F_COUNT) {
             if (noise_mat < 0) continue;
             for (uint32_t q = 0; q < n; q++)

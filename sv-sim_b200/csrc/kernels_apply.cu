@@ -1,9 +1,7 @@
 // Gate-application kernels for sm_100a.
 //
-//  * k_eop_pairs / k_cx : the per-gate engine.  One launch per elementary op, one
-//    streaming sweep over the affected amplitudes with 128-bit complex<double> (64-bit
-//    complex<float>) loads — the work of one OP_HEAD ... OP_TAIL block of the
-//    reference (svsim/src/svsim_nvgpu_sin.cuh:640-651) without its grid barrier.
+//  * the per-gate engine (k_eop_pairs / k_cx) lives in kernels_pergate.cu, which is
+//    compiled without FMA contraction.
 //  * k_staged : the staged engine.  One launch per pass of the planner; every CTA owns
 //    one tile of 2^M amplitudes (the M local qubits of the pass), keeps it in registers
 //    (16 amplitudes per thread) and applies all ops of the pass to it, re-distributing
@@ -16,107 +14,12 @@
 
 namespace svb {
 
-// ---------------------------------------------------------------------------------
-// per-gate engine
-// ---------------------------------------------------------------------------------
-// Each thread takes PG_UNROLL items per iteration (items u * stride apart, so a warp's
-// accesses stay coalesced) and issues all their loads before any arithmetic: more bytes
-// in flight per thread than one pair at a time.
-constexpr int PG_UNROLL = 4;
-
-template <typename T>
-__global__ void __launch_bounds__(256)
-k_eop_pairs(typename VecOf<T>::type* __restrict__ sv, uint64_t half, int q, int form,
-            Coef<T> c)
-{
-    using V = typename VecOf<T>::type;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t qd = 1ull << q;
-    const bool diag = form_is_diag(form);
-    const bool both = !diag || form == F_DIAG;     // diagonal forms other than D leave |0> alone
-    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < half;
-         i0 += PG_UNROLL * stride) {
-        V a0[PG_UNROLL], a1[PG_UNROLL];
-        uint64_t p0[PG_UNROLL];
-#pragma unroll
-        for (int u = 0; u < PG_UNROLL; u++) {
-            const uint64_t i = i0 + (uint64_t)u * stride;
-            p0[u] = insert_zero(i < half ? i : 0, q);
-            if (i < half) {
-                a1[u] = sv[p0[u] | qd];
-                if (both) a0[u] = sv[p0[u]];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < PG_UNROLL; u++) {
-            if (i0 + (uint64_t)u * stride >= half) continue;
-            if (diag) {
-                diag_one<T>(form, c, a1[u]);
-                if (form == F_DIAG) diag_zero<T>(form, c, a0[u]);
-            } else {
-                dense_pair<T>(form, c, a0[u], a1[u]);
-            }
-            sv[p0[u] | qd] = a1[u];
-            if (both) sv[p0[u]] = a0[u];
-        }
-    }
-}
-
-// CX_GATE :779-811 — only the quarter of the state with ctrl = 1 moves.
-template <typename T>
-__global__ void __launch_bounds__(256)
-k_cx(typename VecOf<T>::type* __restrict__ sv, uint64_t quarter, int c, int t)
-{
-    using V = typename VecOf<T>::type;
-    const int lo = c < t ? c : t, hi = c < t ? t : c;
-    const uint64_t cd = 1ull << c, td = 1ull << t;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < quarter;
-         i0 += PG_UNROLL * stride) {
-        V a0[PG_UNROLL], a1[PG_UNROLL];
-        uint64_t b[PG_UNROLL];
-#pragma unroll
-        for (int u = 0; u < PG_UNROLL; u++) {
-            const uint64_t i = i0 + (uint64_t)u * stride;
-            b[u] = insert_zero(insert_zero(i < quarter ? i : 0, lo), hi) | cd;
-            if (i < quarter) {
-                a0[u] = sv[b[u]];
-                a1[u] = sv[b[u] | td];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < PG_UNROLL; u++) {
-            if (i0 + (uint64_t)u * stride >= quarter) continue;
-            sv[b[u]] = a1[u];
-            sv[b[u] | td] = a0[u];
-        }
-    }
-}
-
 static unsigned grid_for(uint64_t items, int threads)
 {
     // enough CTAs to fill 148 SMs several times over, grid-stride beyond that
-    const uint64_t need = (items + (uint64_t)threads * PG_UNROLL - 1) / ((uint64_t)threads * PG_UNROLL);
+    const uint64_t need = (items + (uint64_t)threads * 4 - 1) / ((uint64_t)threads * 4);
     const uint64_t cap = 148ull * 8;
     return (unsigned)(need < cap ? (need > 0 ? need : 1) : cap);
-}
-
-template <typename T>
-cudaError_t launch_eop(void* state, int n, const EOp& op, cudaStream_t s)
-{
-    using V = typename VecOf<T>::type;
-    V* sv = static_cast<V*>(state);
-    if (op.form == F_CX) {
-        if (n < 2) return cudaErrorInvalidValue;
-        const uint64_t quarter = 1ull << (n - 2);
-        k_cx<T><<<grid_for(quarter, 256), 256, 0, s>>>(sv, quarter, (int)op.c, (int)op.q);
-    } else {
-        const uint64_t half = 1ull << (n - 1);
-        Coef<T> c;
-        for (int i = 0; i < 8; i++) c.m[i] = static_cast<T>(op.m[i]);
-        k_eop_pairs<T><<<grid_for(half, 256), 256, 0, s>>>(sv, half, (int)op.q, (int)op.form, c);
-    }
-    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------
@@ -429,7 +332,6 @@ cudaError_t launch_soa_merge(void* state, uint64_t first, uint64_t count, const 
 }
 
 #define SVB_INSTANTIATE(T)                                                                   \
-    template cudaError_t launch_eop<T>(void*, int, const EOp&, cudaStream_t);                \
     template cudaError_t launch_staged_pass<T>(void*, int, int, int, const DevPlanBuffers&,   \
                                                cudaStream_t);                                \
     template cudaError_t launch_reset<T>(void*, int, cudaStream_t);                          \

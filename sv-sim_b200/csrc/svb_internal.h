@@ -342,20 +342,50 @@ cudaError_t launch_soa_merge(void* state, uint64_t first, uint64_t count,
 // Reductions and measurement (measure.cu)
 // ---------------------------------------------------------------------------------
 struct MeasureScratch {
-    double* block_sums = nullptr;   // per block of 2^MEAS_BLOCK_BITS amplitudes
-    double* block_prefix = nullptr; // exclusive prefix of block_sums (+ total at end)
+    double* cdf = nullptr;          // measurement workspace, measure_layout(n).doubles doubles
     double* uniforms = nullptr;
     uint64_t* samples = nullptr;
     double* partial = nullptr;      // reduction partials
-    size_t cap_blocks = 0, cap_shots = 0, cap_partial = 0;
+    size_t cap_doubles = 0, cap_shots = 0, cap_partial = 0;
 };
-constexpr int MEAS_BLOCK_BITS = 12;
+constexpr int MEAS_BLOCK_BITS = 12;   // 4096 amplitudes per block
+constexpr int MEAS_SUPER_BITS = 6;    // 64 blocks per superblock
 
+// Offsets (in doubles) of the measurement workspace's arrays for a 2^n state.
+struct MeasureLayout {
+    uint64_t nblocks = 0, nsuper = 0;
+    uint64_t off_entry = 0, off_start = 0, off_sentry = 0, off_sstart = 0, off_desc = 0;
+    uint64_t doubles = 0;
+};
+constexpr MeasureLayout measure_layout(int n)
+{
+    MeasureLayout L;
+    const uint64_t dim = 1ull << n;
+    L.nblocks = (dim + (1ull << MEAS_BLOCK_BITS) - 1) >> MEAS_BLOCK_BITS;
+    L.nsuper = (L.nblocks + (1ull << MEAS_SUPER_BITS) - 1) >> MEAS_SUPER_BITS;
+    // block entries | block starts (+ total) | superblock entries |
+    // superblock starts (+ total) | descent flags (two 32-bit flags per double)
+    L.off_entry = 0;
+    L.off_start = L.off_entry + L.nblocks;
+    L.off_sentry = L.off_start + L.nblocks + 1;
+    L.off_sstart = L.off_sentry + L.nsuper;
+    L.off_desc = L.off_sstart + L.nsuper + 1;
+    L.doubles = L.off_desc + (L.nsuper + 1) / 2;
+    return L;
+}
+
+// Samples with the reference's rule on its sequential FP64 prefix, bit for bit
+// (measure.cu).  Fails with cudaErrorInvalidValue if scr.cdf holds fewer than
+// measure_layout(n).doubles doubles.
 template <typename T>
 cudaError_t measure_device(const void* state, int n, const double* d_uniforms, uint32_t shots,
                            uint64_t* d_samples, double* d_total, MeasureScratch& scr,
                            cudaStream_t s);
 size_t measure_scratch_doubles(int n);
+// sum |a|^2 in FP64, summed hierarchically (4096-amplitude blocks, then their scan): the
+// accurate norm, not the reference's sequential total (which measure_device reports)
+template <typename T>
+cudaError_t norm2_device(const void* state, int n, double* d_total, MeasureScratch& scr, cudaStream_t s);
 template <typename T>
 cudaError_t expectation_device(const void* state, int n, const svb_pauli_term* d_terms,
                                int n_terms, double* d_out, double* d_partial, cudaStream_t s);
@@ -374,10 +404,15 @@ struct GrowBuf {
 };
 cudaError_t grow(GrowBuf& b, size_t bytes);
 void release(GrowBuf& b);
+cudaError_t grow_host(GrowBuf& b, size_t bytes);   // pinned host memory (cudaMallocHost)
+void release_host(GrowBuf& b);
 
 // Scratch of svb_adjoint, reused across calls on the same handle.
 struct AdjScratch {
     GrowBuf lam, partial, results, terms, final_state;
+    GrowBuf host_stage;                             // pinned host staging of plans and results
+    int ck_count = -1;                              // checkpoints chosen for ck_bytes-sized states
+    size_t ck_bytes = 0;
     GrowBuf plan_passes, plan_stages, plan_ops;     // forward segments' staged plans
     GrowBuf pair_passes, pair_ops, pair_layouts, pair_gates;   // or their pair plans
     GrowBuf rev_passes, rev_ops, rev_slots;         // the tiled reverse sweep's plan

@@ -80,10 +80,13 @@ _SIGS = {
                            _dp], ctypes.c_int),
     "svb_dm_create": ([ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
     "svb_dm_set_circuit": ([_vp, _vp, ctypes.c_size_t, _dp, ctypes.c_uint32], ctypes.c_int),
+    "svb_dm_set_circuit_superops": ([_vp, _vp, ctypes.c_size_t, _dp, ctypes.c_uint32, _vp, ctypes.c_size_t],
+                                    ctypes.c_int),
     "svb_dm_probabilities": ([_vp, _dp], ctypes.c_int),
     "svb_last_error": ([], ctypes.c_char_p),
     "svb_version": ([], ctypes.c_char_p),
     "svb_fp64_mma_peak": ([ctypes.c_int, _dp], ctypes.c_int),
+    "svb_l2_copy_peak": ([ctypes.c_int, _dp], ctypes.c_int),
 }
 
 
@@ -116,6 +119,13 @@ def fp64_mma_peak(device: int = 0) -> float:
     """FP64 tensor-core rate in TFLOP/s measured on `device` (svb_fp64_mma_peak)."""
     v = ctypes.c_double()
     check(lib().svb_fp64_mma_peak(device, ctypes.byref(v)))
+    return v.value
+
+
+def l2_copy_peak(device: int = 0) -> float:
+    """L2 copy bandwidth in GB/s measured on `device` (svb_l2_copy_peak)."""
+    v = ctypes.c_double()
+    check(lib().svb_l2_copy_peak(device, ctypes.byref(v)))
     return v.value
 
 

@@ -26,6 +26,11 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3"
                      "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 
 
+# Per-source extra flags.  The per-gate engine keeps every rounding of the reference's
+# CPU arithmetic (no fused multiply-add), so its FP64 states are bit-identical to it.
+EXTRA_FLAGS = {"kernels_pergate.cu": ["-fmad=false"]}
+
+
 def nvcc() -> str:
     for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
         if cand and os.path.exists(cand):
@@ -53,7 +58,7 @@ def _compile(src: str, verbose: bool) -> str:
     newest = max([_mtime(src)] + [_mtime(h) for h in headers()])
     if _mtime(obj) >= newest:
         return obj
-    cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + NVCC_FLAGS + EXTRA_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -87,7 +92,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
 def ptxas_report(src_name: str) -> str:
     """Register / shared-memory usage of one source (nvcc -Xptxas -v)."""
     src = os.path.join(CSRC, src_name)
-    cmd = [nvcc()] + NVCC_FLAGS + ["-Xptxas", "-v", "-c", src, "-o", os.devnull]
+    cmd = [nvcc()] + NVCC_FLAGS + EXTRA_FLAGS.get(src_name, []) + ["-Xptxas", "-v", "-c", src, "-o", os.devnull]
     res = subprocess.run(cmd, capture_output=True, text=True)
     return res.stdout + res.stderr
 

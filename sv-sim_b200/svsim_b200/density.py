@@ -13,7 +13,9 @@ import ctypes
 import numpy as np
 
 from . import _native as nat
-from .gates import GATE_DTYPE
+from .gates import GATE_DTYPE, OP
+
+SUPEROP_DTYPE = np.dtype([("op", np.uint32), ("reserved", np.uint32), ("m", np.float64, (32,))])
 
 
 def depolarizing(p: float):
@@ -23,6 +25,27 @@ def depolarizing(p: float):
     y = np.array([[0, -1j], [1j, 0]])
     z = np.diag([1, -1])
     return [np.sqrt(1 - p) * i, np.sqrt(p / 3) * x, np.sqrt(p / 3) * y, np.sqrt(p / 3) * z]
+
+
+def pauli_channel(p_i: float, p_x: float, p_y: float, p_z: float):
+    """rho -> p_i rho + p_x X rho X + p_y Y rho Y + p_z Z rho Z."""
+    i = np.eye(2)
+    x = np.array([[0, 1], [1, 0]])
+    y = np.array([[0, -1j], [1j, 0]])
+    z = np.diag([1, -1])
+    return [np.sqrt(p_i) * i, np.sqrt(p_x) * x, np.sqrt(p_y) * y, np.sqrt(p_z) * z]
+
+
+def superoperator(kraus, unitary=None):
+    """4x4 superoperator of rho -> sum_k K_k (U rho U^dagger) K_k^dagger in the reference's
+    table order (svsim_qsharp_noise/noise_gate_*.cuh): entry [r, c] with r = 2 i + j for
+    rho[i][j], so that rho'_r = sum_c S[r, c] rho_c."""
+    u = np.eye(2) if unitary is None else np.asarray(unitary, dtype=np.complex128)
+    s = np.zeros((4, 4), dtype=np.complex128)
+    for k in kraus:
+        m = np.asarray(k, dtype=np.complex128) @ u
+        s += np.kron(m, m.conj())
+    return s
 
 
 def amplitude_damping(gamma: float):
@@ -47,13 +70,23 @@ class DensityMatrix:
         self.handle.precision = nat.SVB_FP64
         self.n = n_qubits
 
-    def set_circuit(self, gates, kraus=None):
+    def set_circuit(self, gates, kraus=None, superops=None):
+        """`kraus`: one-qubit channel applied after every gate to each qubit it touches.
+        `superops`: {op name or enum value: 4x4 complex superoperator in the reference's
+        table order (see ``superoperator``)} for one-qubit ops; such a gate is applied as
+        its superoperator alone, noise included, like the reference's noisy gates."""
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
         ks = [np.asarray(k, dtype=np.complex128).reshape(2, 2) for k in (kraus or [])]
         flat = np.zeros(max(1, 8 * len(ks)))
         for i, k in enumerate(ks):
             flat[8 * i:8 * i + 8] = np.stack([k.real, k.imag], axis=-1).reshape(-1)
-        nat.check(nat.lib().svb_dm_set_circuit(self.handle.ptr, g.ctypes.data, len(g), nat.dptr(flat), len(ks)))
+        so = np.zeros(len(superops or {}), dtype=SUPEROP_DTYPE)
+        for i, (op, m) in enumerate((superops or {}).items()):
+            m = np.asarray(m, dtype=np.complex128).reshape(4, 4)
+            so[i]["op"] = OP[op] if isinstance(op, str) else int(op)
+            so[i]["m"] = np.stack([m.real, m.imag], axis=-1).reshape(-1)
+        nat.check(nat.lib().svb_dm_set_circuit_superops(self.handle.ptr, g.ctypes.data, len(g), nat.dptr(flat),
+                                                        len(ks), so.ctypes.data if len(so) else None, len(so)))
         return self
 
     def run(self):

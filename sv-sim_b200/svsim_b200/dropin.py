@@ -11,8 +11,10 @@ nothing is copied into this repository):
 
 They include their headers as "config.hpp" or "../src/svsim_nvgpu_sin.cuh"; compiling
 from stdin inside a scratch directory whose ../src holds links to the drop-in headers
-makes those quoted includes resolve to the drop-in.  When the reference tree is not
-present (e.g. on a GPU box) the previously built artefacts are used as they are.
+makes those quoted includes resolve to the drop-in.  The reference tree's location is
+the caller's argument or the SVSIM_REFERENCE environment variable; when neither names an
+existing tree (e.g. on a machine without the reference) the previously built artefacts
+are used as they are.
 """
 from __future__ import annotations
 
@@ -22,7 +24,6 @@ import sysconfig
 
 from .build import LIB_DIR, LIB_PATH, PROJECT, ROOT
 
-REF_SRC = "/root/reference/svsim"
 DROPIN = os.path.join(ROOT, "include", "svsim_dropin")
 SCRATCH = os.path.join(PROJECT, "_build", "dropin")
 EXT = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
@@ -56,8 +57,12 @@ def _compile_stdin(source: str, out: str, extra: list[str]):
         subprocess.run(cmd, stdin=f, cwd=work, check=True)
 
 
-def build_python_module(force: bool = False) -> str | None:
-    if not os.path.isdir(REF_SRC):
+def build_python_module(force: bool = False, reference: str | None = None) -> str | None:
+    """Builds the three reference front ends from the reference tree at `reference`
+    (default: $SVSIM_REFERENCE) against the drop-in headers."""
+    reference = reference or os.environ.get("SVSIM_REFERENCE", "")
+    REF_SRC = os.path.join(reference, "svsim") if reference else ""
+    if not REF_SRC or not os.path.isdir(REF_SRC):
         return MODULE if os.path.exists(MODULE) else None
     import pybind11
     srcs = {

@@ -97,6 +97,34 @@ def test_every_op_matches_reference_states():
         assert np.max(np.abs(im - d["im"][i])) <= 1e-14, name
 
 
+def test_per_gate_engine_is_bit_identical_to_the_reference_cpu():
+    """The per-gate engine is compiled without FMA contraction and evaluates the reference's
+    gate expressions in the reference's order, so its FP64 states equal the reference CPU
+    backend's bit for bit: every op (golden states of svsim_cpu_sin.hpp) and the 14 unit
+    tests' circuits."""
+    nat = native()
+    d = load_golden("all_ops_n6.npz")
+    bad = []
+    for i, name in enumerate(d["names"]):
+        g = d["gates"][d["gate_offsets"][i]:d["gate_offsets"][i + 1]]
+        _, re, im = run_gpu(6, g, nat.ENGINE_PER_GATE)
+        if not (np.array_equal(re, d["re"][i]) and np.array_equal(im, d["im"][i])):
+            bad.append(str(name))
+    assert not bad, sorted(set(bad))
+    b = load_golden("brickwork.npz")
+    _, re, im = run_gpu(12, b["gates12"], nat.ENGINE_PER_GATE)
+    assert np.array_equal(re, b["re12"]) and np.array_equal(im, b["im12"])
+
+
+@pytest.mark.parametrize("n", [13, 21])
+def test_per_gate_engine_is_bit_identical_to_the_oracle(oracle, n):
+    nat = native()
+    g = mixed_circuit(n, 2, seed=n)
+    ore, oim = oracle.run(n, g)
+    _, re, im = run_gpu(n, g, nat.ENGINE_PER_GATE)
+    assert np.array_equal(re, ore) and np.array_equal(im, oim)
+
+
 @pytest.mark.parametrize("engine_idx", range(4))
 def test_every_op_all_engines(oracle, engine_idx):
     n = 12
