@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--engine", choices=["staged", "pairs"], default="pairs",
                     help="FP64 engine of the headline step")
     ap.add_argument("--form", choices=["headline", "pergate", "fused", "qaoa", "capacity", "adjoint", "density",
-                                       "config1"],
+                                       "config1", "tuning", "batch", "refgpu"],
                     default="headline",
                     help="headline: the FP64 n=30 step (the measured line); the others run one "
                          "secondary form alone (for profiling and capacity runs)")
@@ -576,11 +576,17 @@ def run_form(args):
         return
     torch.cuda.set_device(local)
     if args.form == "adjoint":
-        res = adjoint_form(local)
+        res = adjoint_form(local, reps=max(1, args.steps), warmup=args.warmup, shift=not args.no_baseline)
     elif args.form == "density":
         res = density_form(local)
     elif args.form == "config1":
         res = config1_form(local)
+    elif args.form == "tuning":
+        res = tuning_form(local)
+    elif args.form == "batch":
+        res = batch_form(local)
+    elif args.form == "refgpu":
+        res = reference_gpu_form(local)
     elif args.form == "pergate":
         from svsim_b200 import circuits
         res = per_gate_form(local, circuits.random_matching_circuit(args.qubits, DEPTH, seed=SEED), n=args.qubits)
@@ -732,6 +738,104 @@ def fused_form(device, circuit, k=None, reps=3, n=N_QUBITS):
     return out
 
 
+def tuning_form(device):
+    """The autotuner on the headline circuit (FP64 and FP32 states of n=30): the candidate
+    engines timed on the first 360 gates, the choice next to the static default."""
+    import torch
+    from svsim_b200 import circuits, _native as nat
+    g = circuits.random_matching_circuit(N_QUBITS, DEPTH, seed=SEED)
+    names = {0: "auto", 1: "per_gate", 2: "staged", 3: "fused", 4: "pairs"}
+    out = {}
+    for prec, key in ((nat.SVB_FP64, "fp64"), (nat.SVB_FP32, "fp32")):
+        h = nat.Handle(N_QUBITS, device, prec)
+        t0 = time.perf_counter()
+        r = h.autotune(g)
+        out[key] = {"chosen": names.get(r.engine, r.engine), "tile_bits": r.tile_bits,
+                    "fusion_width": r.fusion_width, "candidates": r.candidates,
+                    "chosen_ms_on_prefix": r.best_ms, "default_ms_on_prefix": r.default_ms,
+                    "timed_gates": int(r.timed_gates), "tuning_s": time.perf_counter() - t0}
+        h.close()
+        torch.cuda.empty_cache()
+    return out
+
+
+def batch_form(device, reps=5):
+    """Batched circuits in one graph-replayed persistent launch (svb_cbatch_*): 64
+    parameter points of the n=20, 480-parameter ansatz with their energies, and 128
+    random circuits with n ~ U{10..22}; the autotuned tile/block choice next to the fixed
+    default (12-qubit tiles, 512 threads)."""
+    import torch
+    from svsim_b200 import circuits, _native as nat
+    pc = circuits.hardware_efficient_ansatz()
+    terms = circuits.zz_x_hamiltonian(20)
+    pts = np.random.default_rng(5).uniform(-np.pi, np.pi, size=(64, len(pc.params)))
+    rng = np.random.default_rng(6)
+    mixed = []
+    for i in range(128):
+        n = int(rng.integers(10, 23))
+        mixed.append((n, circuits.random_matching_circuit(n, 10, seed=1000 + i)))
+    out = {}
+    for name, batch, tb in (("ansatz_points_64", [(20, pc.evaluated(p)) for p in pts], None),
+                            ("random_mixed_128", mixed, None)):
+        res = {}
+        for label, tile in (("tuned", 0), ("fixed_tile12", 12)):
+            t0 = time.perf_counter()
+            b = nat.CircuitBatch(batch, [terms] * len(batch) if name.startswith("ansatz") else None,
+                                 device=device, tile_bits=tile)
+            setup = time.perf_counter() - t0
+            b.run()
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                b.run()
+            sec = (time.perf_counter() - t0) / reps
+            st = b.info()
+            gates = sum(len(g) for _, g in batch)
+            res[label] = {"circuits_per_s": len(batch) / sec, "ms_per_batch": sec * 1e3,
+                          "gates_per_s": gates / sec, "tile_bits": int(st.tile_bits), "threads": int(st.threads),
+                          "phases": int(st.n_phases), "graphed": bool(st.graphed), "grid": int(st.grid),
+                          "state_gbs": st.moved_bytes / sec / 1e9, "setup_s": setup}
+            b.close()
+            torch.cuda.empty_cache()
+        out[name] = res
+    out["timing"] = "wall clock of svb_cbatch_run (graph replay, energies back to the host)"
+    return out
+
+
+def reference_gpu_form(device, reps=10):
+    """Context only (the timed reference arm is the CPU path): the reference's own
+    single-GPU kernel (svsim/src/svsim_nvgpu_sin.cuh, built for sm_100a by oracle/Makefile
+    into oracle/_ref/ref_gpu_driver) on this B200, timed by its own event timer around
+    the cooperative kernel (sim() prints it), beside this engine on the same circuits:
+    the n=16 brickwork (470 gates) and the n=26 random-matching circuit, depth 40."""
+    import tempfile
+    from svsim_b200 import circuits
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_driver")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_gpu_driver not built (reference tree absent at build time)"}
+    out = {}
+    for name, n, g in (("brickwork_n16", 16, circuits.brickwork_circuit(16, 20, seed=1234)),
+                       ("matching_n26_depth40", 26, circuits.random_matching_circuit(26, DEPTH, seed=SEED))):
+        with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
+            g.tofile(f)
+            path = f.name
+        try:
+            env = dict(os.environ, CUDA_VISIBLE_DEVICES=str(device))
+            r = subprocess.run([exe, path, str(n), str(reps)], capture_output=True, text=True, timeout=300, env=env)
+        finally:
+            os.unlink(path)
+        ms = [float(x.split("sim:")[1].split("ms")[0]) for x in r.stdout.splitlines() if "sim:" in x]
+        if r.returncode != 0 or not ms:
+            out[name] = {"error": f"rc={r.returncode}", "stderr": r.stderr[-300:]}
+            continue
+        best = float(np.median(ms[1:] if len(ms) > 1 else ms))
+        out[name] = {"gates": len(g), "ms_per_circuit": best, "gates_per_s": len(g) / (best / 1e3),
+                     "runs": len(ms)}
+    out["what"] = ("reference svsim_nvgpu_sin.cuh compiled for sm_100a (its config.mk flags); "
+                   "sim() event time of the cooperative kernel, median of the runs after the first")
+    return out
+
+
 def density_form(device, n=14, depth=10, reps=3):
     """Density matrix of n=14 qubits (a 28-qubit FP64 vector, 4 GiB) through a depth-10
     random-matching circuit with a depolarizing channel (p = 0.01) after every gate on each
@@ -765,18 +869,24 @@ def density_form(device, n=14, depth=10, reps=3):
     return out
 
 
-def adjoint_form(device, reps=5):
-    """Adjoint gradients of the n=20, 480-parameter ansatz against parameter shift on the
-    same GPU (2 circuits per parameter, timed on 48 of 480 and scaled)."""
+def adjoint_form(device, reps=5, warmup=1, shift=True):
+    """Adjoint gradients of the n=20, 480-parameter ansatz (svb_adjoint, wall clock per
+    call: host lowering and planning included) against parameter shift on the same GPU
+    (2 circuits per parameter, timed on 48 of 480 and scaled; skipped with shift=False)."""
     from svsim_b200 import circuits, _native as nat
     pc = circuits.hardware_efficient_ansatz()
     terms = circuits.zz_x_hamiltonian(20)
     ha = nat.Handle(20, device, nat.SVB_FP64)
-    ha.adjoint(pc.gates, pc.binding, 480, terms)
+    for _ in range(max(1, warmup)):
+        ha.adjoint(pc.gates, pc.binding, 480, terms)
     t0 = time.perf_counter()
     for _ in range(reps):
         ha.adjoint(pc.gates, pc.binding, 480, terms)
     t_adj = (time.perf_counter() - t0) / reps
+    out = {"grads_per_s": 1.0 / t_adj, "ms_per_gradient": t_adj * 1e3,
+           "workload": "n=20, 12 layers RY+RZ+CX ring, 720 gates, P=480, H = sum ZZ + 0.5 sum X"}
+    if not shift:
+        return out
     hp = nat.Handle(20, device, nat.SVB_FP64)
     nshift = 48
     t0 = time.perf_counter()
@@ -789,10 +899,9 @@ def adjoint_form(device, reps=5):
             hp.run()
             hp.expectation(terms)
     t_shift = (time.perf_counter() - t0) / nshift * 480
-    return {"grads_per_s": 1.0 / t_adj, "param_shift_grads_per_s": 1.0 / t_shift,
-            "speedup_vs_param_shift": t_shift / t_adj,
-            "workload": "n=20, 12 layers RY+RZ+CX ring, 720 gates, P=480, H = sum ZZ + 0.5 sum X",
-            "param_shift_sample": f"{nshift} of 480 parameters timed, scaled"}
+    out.update({"param_shift_grads_per_s": 1.0 / t_shift, "speedup_vs_param_shift": t_shift / t_adj,
+                "param_shift_sample": f"{nshift} of 480 parameters timed, scaled"})
+    return out
 
 
 def secondary_forms(device, circuit):
@@ -810,6 +919,9 @@ def secondary_forms(device, circuit):
     forms["qaoa_batch_fp32"] = qaoa_form(device, 512, "fp32")
     forms["capacity"] = capacity_form(device)
     forms["adjoint"] = adjoint_form(device)
+    forms["autotune"] = tuning_form(device)
+    forms["reference_gpu_kernel"] = reference_gpu_form(device)
+    forms["batched_circuits"] = batch_form(device)
     forms["density_matrix"] = density_form(device)
     return forms
 

@@ -125,6 +125,28 @@ svb_status svb_clear_circuit(svb_sim* sim);
  * fused engines. */
 svb_status svb_set_engine(svb_sim* sim, int engine, int tile_bits, int fusion_width);
 
+/* Result of svb_autotune. */
+typedef struct svb_tune_result {
+    int engine;               /* svb_engine chosen */
+    int tile_bits;            /* staged engine: local qubits per tile (0 otherwise) */
+    int fusion_width;         /* fused engine: qubits per fused block (0 otherwise) */
+    int candidates;           /* configurations timed */
+    double best_ms;           /* time of the chosen configuration on the timed gates */
+    double default_ms;        /* time of the static AUTO choice on the same gates (-1 if it failed) */
+    uint64_t timed_gates;     /* gates timed: the circuit's first min(n_gates, 360) */
+} svb_tune_result;
+
+/* Autotuner (no reference counterpart; the reference fixes its launch shape,
+ * svsim_nvgpu_sin.cuh:309-316, config.hpp:48): times every engine configuration that can
+ * run the circuit on this handle (per-gate for n <= 26; staged at each tile size; the pair
+ * engine for FP64 or the fused engine at k = 3..5 for FP32, when the circuit has no SRN)
+ * on its first min(n_gates, 360) gates, one warm-up and one timed run each, and keeps the
+ * fastest for this circuit structure (qubit count, precision, and the ops and qubits of
+ * every elementary op; angles ignored): from then on svb_set_circuit with
+ * SVB_ENGINE_AUTO picks it for any circuit of that structure on this device.  The handle
+ * ends with `gates` set as its circuit and the state at |0..0>.  `out` may be NULL. */
+svb_status svb_autotune(svb_sim* sim, const svb_gate* gates, size_t n_gates, svb_tune_result* out);
+
 /* Statistics of the current plan. */
 svb_status svb_get_plan_info(const svb_sim* sim, svb_plan_info* out);
 

@@ -36,7 +36,7 @@ def build(reference: bool = True) -> None:
     """Build the restatement, and the reference backends when the reference tree exists."""
     targets = ["oracle"]
     if reference and os.path.isdir(os.path.join(REFERENCE, "svsim", "src")):
-        targets.append("ref")
+        targets += ["ref", "ref_gpu"]
     subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE}"] + targets, check=True)
 
 

@@ -8,6 +8,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <array>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "svb_internal.h"
@@ -466,6 +469,27 @@ svb_status svb_set_circuit(svb_sim* s, const svb_gate* gates, size_t n_gates)
 
 namespace svb {
 
+// ---- the autotuner's choices, per circuit structure --------------------------------
+// Key: device, qubit count, precision and an FNV-1a hash of the elementary ops' forms and
+// qubits (angles left out, so a variational loop reuses one choice).
+struct TuneChoice {
+    int engine = SVB_ENGINE_AUTO, tile_bits = 0, fusion_width = 0;
+};
+std::mutex g_tune_mutex;
+std::map<std::array<uint64_t, 4>, TuneChoice> g_tuned;
+
+std::array<uint64_t, 4> structure_key(const Sim* s, const std::vector<EOp>& eops)
+{
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
+    for (const EOp& e : eops) {
+        mix(e.form);
+        mix(e.q);
+        mix(e.c);
+    }
+    return {(uint64_t)s->device, (uint64_t)s->n | ((uint64_t)s->precision << 32), (uint64_t)eops.size(), h};
+}
+
 svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* gates, size_t n_gates, double sweeps)
 {
     SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
@@ -480,7 +504,18 @@ svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* g
 
     int engine = s->engine_req;
     const int n = (int)s->n;
-    const int M = pick_tile_bits(s);
+    int M = pick_tile_bits(s);
+    int fusion = s->fusion_req;
+    if (engine == SVB_ENGINE_AUTO && !has_m4 && !s->dm_qubits) {
+        // a choice of svb_autotune for this circuit structure, if there is one
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tuned.find(structure_key(s, s->eops));
+        if (it != g_tuned.end()) {
+            engine = it->second.engine;
+            if (it->second.tile_bits) M = it->second.tile_bits;
+            if (it->second.fusion_width) fusion = it->second.fusion_width;
+        }
+    }
     if (has_m4) {
         // general 4x4 blocks: the pair engine, or per-gate sweeps below its tile
         if (engine == SVB_ENGINE_AUTO)
@@ -532,7 +567,7 @@ svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* g
     s->info.model_bytes = 2.0 * sb * sweeps;
     s->info.engine = engine;
     if (engine == SVB_ENGINE_FUSED) {
-        const int k = s->fusion_req ? s->fusion_req : FT_MAX_K;
+        const int k = fusion ? fusion : FT_MAX_K;
         plan_fused(s->eops, n, k, s->fused);
         const FusedPlan& F = s->fused;
         SVB_CUDA(cudaMalloc(&s->dfused.passes, std::max<size_t>(1, F.passes.size()) * sizeof(FusedPass)),
@@ -865,3 +900,100 @@ svb_status svb_expectation(svb_sim* s, const svb_pauli_term* terms, size_t n_ter
 }
 
 }  // extern "C"
+
+extern "C" svb_status svb_autotune(svb_sim* s, const svb_gate* gates, size_t n_gates, svb_tune_result* out)
+{
+    using namespace svb;
+    if (!s || (n_gates && !gates)) return invalid("svb_autotune: NULL argument");
+    if (s->dm_qubits) return invalid("svb_autotune: not for density-matrix handles");
+    SVB_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+    std::vector<EOp> eops;
+    double sweeps = 0;
+    svb_status st = validate_and_lower(s, gates, n_gates, eops, &sweeps);
+    if (st != SVB_OK) return st;
+    const int n = (int)s->n;
+    const bool fp64 = s->precision == SVB_FP64;
+    const bool matrices = fusable(eops);
+    const auto key = structure_key(s, eops);
+    // candidates: (engine, tile bits, fusion width)
+    std::vector<TuneChoice> cands;
+    if (n <= 26) cands.push_back({SVB_ENGINE_PER_GATE, 0, 0});
+    for (int M = fp64 ? 10 : 11; M <= (fp64 ? 12 : 13); M++)
+        if (n >= M) cands.push_back({SVB_ENGINE_STAGED, M, 0});
+    if (n >= PR_TILE_BITS && matrices) {
+        if (fp64) cands.push_back({SVB_ENGINE_PAIRS, 0, 0});
+        else
+            for (int k = FT_MIN_K; k <= FT_MAX_K; k++) cands.push_back({SVB_ENGINE_FUSED, 0, k});
+    }
+    // the prefix timed: the whole circuit up to 360 gates (the choice holds for the structure)
+    const size_t P = std::min<size_t>(n_gates, 360);
+    const int req_e = s->engine_req, req_t = s->tile_bits_req, req_k = s->fusion_req;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned.erase(key);                      // the default choice is timed as well
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    SVB_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
+    SVB_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
+    TuneChoice best;
+    double best_ms = 1e300, default_ms = -1;
+    int tried = 0;
+    // the static default first (engine AUTO with no tuned choice)
+    std::vector<TuneChoice> order = {TuneChoice{}};
+    order.insert(order.end(), cands.begin(), cands.end());
+    for (size_t ci = 0; ci < order.size(); ci++) {
+        const TuneChoice& c = order[ci];
+        s->engine_req = c.engine;
+        s->tile_bits_req = c.tile_bits;
+        s->fusion_req = c.fusion_width;
+        if (svb_set_circuit(s, gates, P) != SVB_OK) continue;
+        svb_reset_state(s);
+        float ms = 0.f;
+        cudaError_t e = svb_run(s, nullptr) == SVB_OK ? cudaSuccess : cudaErrorUnknown;     // warm-up
+        if (e == cudaSuccess) e = cudaEventRecord(e0, nullptr);
+        if (e == cudaSuccess) e = svb_run(s, nullptr) == SVB_OK ? cudaSuccess : cudaErrorUnknown;
+        if (e == cudaSuccess) e = cudaEventRecord(e1, nullptr);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess || svb_synchronize(s) != SVB_OK) {
+            (void)cudaGetLastError();
+            continue;
+        }
+        if (ci == 0) {
+            default_ms = ms;
+            continue;
+        }
+        tried++;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->engine_req = req_e;
+    s->tile_bits_req = req_t;
+    s->fusion_req = req_k;
+    if (tried == 0) {
+        set_error("svb_autotune: no candidate engine could run the circuit");
+        return SVB_ERR_UNSUPPORTED;
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned[key] = best;
+    }
+    if (out) {
+        out->engine = best.engine;
+        out->tile_bits = best.tile_bits;
+        out->fusion_width = best.fusion_width;
+        out->candidates = tried;
+        out->best_ms = best_ms;
+        out->default_ms = default_ms;
+        out->timed_gates = (uint64_t)P;
+    }
+    // the handle ends with the circuit planned for its own engine request (AUTO: the
+    // tuned choice) and the state at |0..0>
+    st = svb_set_circuit(s, gates, n_gates);
+    if (st != SVB_OK) return st;
+    return svb_reset_state(s);
+}

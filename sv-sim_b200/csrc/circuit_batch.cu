@@ -205,8 +205,10 @@ __global__ void __launch_bounds__(512) k_cbatch(CbArgs A)
             const CbCircuit C = A.circ[item.circuit];
             const int M = sp->M;
             const uint32_t TL = 1u << M;
-            uint64_t base = C.state_off;
-            for (int j = 0; j < sp->n_nonlocal; j++) base |= ((item.tile >> j) & 1ull) << sp->nonlocal_q[j];
+            // the tile's offset within the circuit's state (state_off is not aligned to 2^n)
+            uint64_t off = 0;
+            for (int j = 0; j < sp->n_nonlocal; j++) off |= ((item.tile >> j) & 1ull) << sp->nonlocal_q[j];
+            const uint64_t base = C.state_off + off;
             for (uint32_t l = threadIdx.x; l < TL; l += blockDim.x) tile[l] = pool[base + sp->g_lo[l & 63u] + sp->g_hi[l >> 6]];
             __syncthreads();
             for (int o = sp->op_begin; o < sp->op_end; o++) {

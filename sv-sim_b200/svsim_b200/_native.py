@@ -43,6 +43,21 @@ class QaoaStats(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+class TuneResult(ctypes.Structure):
+    _fields_ = [("engine", ctypes.c_int), ("tile_bits", ctypes.c_int), ("fusion_width", ctypes.c_int),
+                ("candidates", ctypes.c_int), ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double),
+                ("timed_gates", ctypes.c_uint64)]
+
+
+class CbatchStats(ctypes.Structure):
+    _fields_ = [("n_circuits", ctypes.c_uint32), ("n_phases", ctypes.c_uint32),
+                ("tile_bits", ctypes.c_uint32), ("threads", ctypes.c_uint32),
+                ("pool_amplitudes", ctypes.c_uint64), ("items", ctypes.c_uint64),
+                ("grid", ctypes.c_uint32), ("graphed", ctypes.c_uint32),
+                ("moved_bytes", ctypes.c_double), ("tuned", ctypes.c_uint32),
+                ("n_passes", ctypes.c_uint32)]
+
+
 _lib = None
 
 _vp = ctypes.c_void_p
@@ -83,6 +98,13 @@ _SIGS = {
     "svb_dm_set_circuit_superops": ([_vp, _vp, ctypes.c_size_t, _dp, ctypes.c_uint32, _vp, ctypes.c_size_t],
                                     ctypes.c_int),
     "svb_dm_probabilities": ([_vp, _dp], ctypes.c_int),
+    "svb_autotune": ([_vp, _vp, ctypes.c_size_t, ctypes.POINTER(TuneResult)], ctypes.c_int),
+    "svb_cbatch_create": ([ctypes.c_int, ctypes.c_int, ctypes.c_uint32, _vp, _vp, _vp, _vp, _vp, ctypes.c_int,
+                           ctypes.POINTER(_vp)], ctypes.c_int),
+    "svb_cbatch_run": ([_vp, _vp, _dp], ctypes.c_int),
+    "svb_cbatch_get_state": ([_vp, ctypes.c_uint32, _dp, _dp], ctypes.c_int),
+    "svb_cbatch_info": ([_vp, ctypes.POINTER(CbatchStats)], ctypes.c_int),
+    "svb_cbatch_destroy": ([_vp], ctypes.c_int),
     "svb_last_error": ([], ctypes.c_char_p),
     "svb_version": ([], ctypes.c_char_p),
     "svb_fp64_mma_peak": ([ctypes.c_int, _dp], ctypes.c_int),
@@ -153,6 +175,14 @@ class Handle:
     # -- wrappers ------------------------------------------------------------------
     def set_engine(self, engine=ENGINE_AUTO, tile_bits=0, fusion_width=0):
         check(lib().svb_set_engine(self.ptr, engine, tile_bits, fusion_width))
+
+    def autotune(self, gates: np.ndarray) -> TuneResult:
+        """Times the engines that can run `gates` and keeps the fastest for circuits of this
+        structure (svb_autotune); the handle ends with `gates` set and the state at |0..0>."""
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        r = TuneResult()
+        check(lib().svb_autotune(self.ptr, g.ctypes.data, len(g), ctypes.byref(r)))
+        return r
 
     def set_circuit(self, gates: np.ndarray):
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
@@ -305,3 +335,70 @@ class QaoaBatch:
         st = QaoaStats()
         check(lib().svb_qaoa_info(self.ptr, ctypes.byref(st)))
         return st
+
+
+class CircuitBatch:
+    """Many independent circuits (each its own qubit count, 1..24) run together by one
+    persistent, graph-replayed launch (svb_cbatch_*), with an optional Pauli-sum energy per
+    circuit.  tile_bits=0 lets the autotuner choose the tile and block sizes."""
+
+    def __init__(self, circuits, terms=None, device: int = 0, precision: int = SVB_FP64, tile_bits: int = 0):
+        """circuits: list of (n_qubits, gate record array); terms: None or a list (one per
+        circuit) of Pauli-term arrays (PAULI_DTYPE) or None."""
+        self.n = np.array([int(c[0]) for c in circuits], dtype=np.uint32)
+        self.gate_arrays = [np.ascontiguousarray(c[1], dtype=GATE_DTYPE) for c in circuits]
+        self.gate_off = np.zeros(len(circuits) + 1, dtype=np.uint64)
+        np.cumsum([len(g) for g in self.gate_arrays], out=self.gate_off[1:])
+        gates = np.ascontiguousarray(np.concatenate(self.gate_arrays) if len(self.gate_arrays) else
+                                     np.zeros(0, dtype=GATE_DTYPE))
+        self._gates = gates
+        toff = None
+        t = None
+        if terms is not None:
+            ts = [np.zeros(0, dtype=PAULI_DTYPE) if x is None else np.ascontiguousarray(x, dtype=PAULI_DTYPE)
+                  for x in terms]
+            toff = np.zeros(len(circuits) + 1, dtype=np.uint64)
+            np.cumsum([len(x) for x in ts], out=toff[1:])
+            t = np.ascontiguousarray(np.concatenate(ts) if ts else np.zeros(0, dtype=PAULI_DTYPE))
+        self._terms, self._toff = t, toff
+        self.ptr = _vp()
+        check(lib().svb_cbatch_create(device, precision, len(circuits), self.n.ctypes.data,
+                                      self.gate_off.ctypes.data, gates.ctypes.data if len(gates) else None,
+                                      toff.ctypes.data if toff is not None else None,
+                                      t.ctypes.data if t is not None and len(t) else None,
+                                      tile_bits, ctypes.byref(self.ptr)))
+
+    def run(self, gates=None) -> np.ndarray:
+        """Energies of every circuit (zeros without terms); `gates`: the concatenated gate
+        records with new angles (same ops and qubits), or None."""
+        e = np.zeros(len(self.n))
+        g = None
+        if gates is not None:
+            g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+            if len(g) != len(self._gates):
+                raise ValueError("gates: the batch's gate count")
+        check(lib().svb_cbatch_run(self.ptr, g.ctypes.data if g is not None else None, dptr(e)))
+        return e
+
+    def state(self, i: int) -> np.ndarray:
+        dim = 1 << int(self.n[i])
+        re = np.empty(dim)
+        im = np.empty(dim)
+        check(lib().svb_cbatch_get_state(self.ptr, i, dptr(re), dptr(im)))
+        return re + 1j * im
+
+    def info(self) -> CbatchStats:
+        st = CbatchStats()
+        check(lib().svb_cbatch_info(self.ptr, ctypes.byref(st)))
+        return st
+
+    def close(self):
+        if self.ptr:
+            lib().svb_cbatch_destroy(self.ptr)
+            self.ptr = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
