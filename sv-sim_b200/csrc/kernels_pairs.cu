@@ -4,11 +4,12 @@
 // 4,096 amplitudes; a thread keeps 16 complex<double> in registers.  In the current
 // layout lane bits 0 and 1 hold the block's two qubits, so the four lanes t with equal
 // t >> 2 hold the four amplitudes a = t & 3 of one "vector", and the 8 lane groups of a
-// warp hold 8 vectors.  For every register slot the block is two MMAs,
-//     D^T = X^T G'^T :  d = mma(re, B0, 0);  d = mma(im, B1, d)
-// (A fragment = the thread's real or imaginary part, k-step 0 / 1; B = the lane's two
-// entries of the real 8x8 form G'), and the 2 accumulator registers a thread gets back are
-// the real and imaginary part of its own output amplitude a' = t & 3.  So the tile never
+// warp hold 8 vectors.  For every two register slots the block is one m16n8k8 f64 MMA,
+//     D^T = X^T G'^T  (16 vectors x 8 outputs = 16 x 8 inputs . 8 x 8)
+// (A fragment = the thread's real parts (K = 0..3) and imaginary parts (K = 4..7) of its
+// two slots; B = the lane's two entries of the real 8x8 form G'), and the 4 accumulator
+// registers a thread gets back are the real and imaginary parts of its own output
+// amplitude a' = t & 3 in both slots.  So the tile never
 // leaves the registers between blocks on the same pair.  A PO_SWAP exchanges a lane bit
 // with a register bit by one warp shuffle per moved word; a PO_LPERM permutes the lane
 // bits by one indexed shuffle of every word; a PO_RELAYOUT sends the tile through shared
@@ -21,11 +22,15 @@ namespace {
 constexpr int PR_THREADS = 1 << (PR_TILE_BITS - RB);    // 256
 constexpr int PR_NR = 1 << RB;                          // 16
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b, double c0, double c1)
+// D (16 x 8) = A (16 x 8) . B (8 x 8), f64.  Lane 4g + t holds A[g][t], A[g+8][t],
+// A[g][t+4], A[g+8][t+4]; B[t][g], B[t+4][g]; and gets D[g][2t], D[g][2t+1], D[g+8][2t],
+// D[g+8][2t+1].
+__device__ __forceinline__ void dmma16(double& d0, double& d1, double& d2, double& d3, double a0, double a1,
+                                       double a2, double a3, double b0, double b1)
 {
-    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};"
-                 : "=d"(d0), "=d"(d1)
-                 : "d"(a), "d"(b), "d"(c0), "d"(c1));
+    asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%10,%10,%10,%10};"
+        : "=d"(d0), "=d"(d1), "=d"(d2), "=d"(d3)
+        : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1), "d"(0.0));
 }
 
 // exchange lane bit L with register bit R: the element at (lane bit i, register bit j)
@@ -149,13 +154,16 @@ k_pairs(double2* __restrict__ sv, const PairPass* __restrict__ passes, const Pai
                 if (op.ncond > 0) var |= (int)((base >> op.cond_q[0]) & 1ull);
                 if (op.ncond > 1) var |= (int)((base >> op.cond_q[1]) & 1ull) << 1;
                 const double2 g = G[(size_t)((int)op.gate - P.gate_begin + var) * 32 + lane];
+                // two register slots per MMA: slot k as rows g, slot k + 1 as rows g + 8;
+                // K = 8 takes the real parts (k < 4) and the imaginary parts (k >= 4)
 #pragma unroll
-                for (int k = 0; k < PR_NR; k++) {
-                    double d0, d1;
-                    dmma(d0, d1, v[k].x, g.x, 0.0, 0.0);
-                    dmma(d0, d1, v[k].y, g.y, d0, d1);
+                for (int k = 0; k < PR_NR; k += 2) {
+                    double d0, d1, d2, d3;
+                    dmma16(d0, d1, d2, d3, v[k].x, v[k + 1].x, v[k].y, v[k + 1].y, g.x, g.y);
                     v[k].x = d0;
                     v[k].y = d1;
+                    v[k + 1].x = d2;
+                    v[k + 1].y = d3;
                 }
             } else if (op.kind == PO_SWAP) {
                 swap_any(v, op.lane, op.reg);
