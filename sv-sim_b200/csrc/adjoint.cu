@@ -80,7 +80,8 @@ struct AdjTilePass {
     int32_t n_nonlocal, op_begin, op_end;
     int32_t n_lslots;          // derivative slots of the pass's ops
     int32_t lslot_begin;       // their global slot numbers: lslots[lslot_begin + local slot]
-    int32_t pad[3];
+    int32_t stage_begin, stage_end;   // k_adj_stages: the pass's register stages
+    int32_t pad;
 };
 static_assert(sizeof(AdjTilePass) % 16 == 0, "AdjTilePass layout");
 
@@ -213,6 +214,253 @@ k_adj_tiles(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTileP
 #pragma unroll
             for (int w = 0; w < WARPS; w++) v += wsum[j * WARPS + w];
             partial[(uint64_t)lslots[P.lslot_begin + j] * tiles + tile] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// ---- the reverse sweep with register stages (tiles of exactly AT_M = 10 qubits) ------
+// The same passes as k_adj_tiles, but inside a pass the ops are grouped into stages whose
+// dense and CX targets lie on 3 "register" positions of the tile: each of 128 threads
+// keeps the 8 amplitudes of psi and of lambda that differ in those positions in
+// registers, applies the stage's ops there, and the tile goes through shared memory once
+// per stage instead of once per op (k_adj_tiles was bound by its shared-memory sweeps:
+// L1 throughput 79%, FP64 pipe 21%).
+constexpr int AS_THREADS = 1 << (AT_M - 3);   // 128
+constexpr int AS_R = 8;                       // amplitudes of each state per thread
+
+struct AdjStage {
+    uint8_t rp[3];      // local positions held in register bits 0..2
+    uint8_t tp[7];      // local positions of thread-index bits 0..6
+    uint8_t pad[6];
+    int32_t op_begin, op_end;
+    int32_t pad2[2];
+};
+static_assert(sizeof(AdjStage) == 32, "AdjStage layout");
+
+enum { AS_LOC_REG = 0, AS_LOC_THREAD = 1, AS_LOC_TILE = 2 };
+
+struct AdjStageOp {
+    uint8_t kind;      // AT_C1, AT_DIAG, AT_CX
+    uint8_t j;         // C1 / CX: register bit of the target; DIAG: bit of the qubit in its location
+    uint8_t c;         // CX: bit of the control in its location
+    uint8_t loc;       // DIAG qubit / CX control: AS_LOC_REG, AS_LOC_THREAD or AS_LOC_TILE
+    uint8_t nd;        // derivative slots (AT_C1)
+    uint8_t pad[3];
+    int32_t lslot;
+    int32_t pad2;
+    double m[8];
+    double dm[3][8];
+};
+static_assert(sizeof(AdjStageOp) % 16 == 0, "AdjStageOp layout");
+
+template <int J>
+__device__ __forceinline__ void as_c1(double2* vp, double2* vl, const Coef<double>& inv, const double (*dm)[8],
+                                      int nd, double* acc)
+{
+#pragma unroll
+    for (int r = 0; r < AS_R; r++) {
+        if (r & (1 << J)) continue;
+        const int r1 = r | (1 << J);
+        double2 s0 = vp[r], s1 = vp[r1];
+        double2 l0 = vl[r], l1 = vl[r1];
+        dense_pair<double>(F_C1, inv, s0, s1);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (d >= nd) break;
+            const double* m = dm[d];
+            const double u0r = m[0] * s0.x - m[1] * s0.y + m[2] * s1.x - m[3] * s1.y;
+            const double u0i = m[0] * s0.y + m[1] * s0.x + m[2] * s1.y + m[3] * s1.x;
+            const double u1r = m[4] * s0.x - m[5] * s0.y + m[6] * s1.x - m[7] * s1.y;
+            const double u1i = m[4] * s0.y + m[5] * s0.x + m[6] * s1.y + m[7] * s1.x;
+            acc[d] += l0.x * u0r + l0.y * u0i + l1.x * u1r + l1.y * u1i;
+        }
+        dense_pair<double>(F_C1, inv, l0, l1);
+        vp[r] = s0;
+        vp[r1] = s1;
+        vl[r] = l0;
+        vl[r1] = l1;
+    }
+}
+
+template <int J>
+__device__ __forceinline__ void as_swap_all(double2* vp, double2* vl)
+{
+#pragma unroll
+    for (int r = 0; r < AS_R; r++) {
+        if (r & (1 << J)) continue;
+        const int r1 = r | (1 << J);
+        const double2 a = vp[r], b = vl[r];
+        vp[r] = vp[r1];
+        vp[r1] = a;
+        vl[r] = vl[r1];
+        vl[r1] = b;
+    }
+}
+
+template <int J, int C>
+__device__ __forceinline__ void as_swap_ctrl(double2* vp, double2* vl)
+{
+#pragma unroll
+    for (int r = 0; r < AS_R; r++) {
+        if ((r & (1 << J)) || !(r & (1 << C))) continue;
+        const int r1 = r | (1 << J);
+        const double2 a = vp[r], b = vl[r];
+        vp[r] = vp[r1];
+        vp[r1] = a;
+        vl[r] = vl[r1];
+        vl[r1] = b;
+    }
+}
+
+template <int J>
+__device__ __forceinline__ void as_diag_reg(double2* vp, double2* vl, const Coef<double>& inv)
+{
+#pragma unroll
+    for (int r = 0; r < AS_R; r++) {
+        if (r & (1 << J)) {
+            diag_one<double>(F_DIAG, inv, vp[r]);
+            diag_one<double>(F_DIAG, inv, vl[r]);
+        } else {
+            diag_zero<double>(F_DIAG, inv, vp[r]);
+            diag_zero<double>(F_DIAG, inv, vl[r]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(AS_THREADS, 3)
+k_adj_stages(double2* __restrict__ psi, double2* __restrict__ lam, const AdjTilePass* __restrict__ passes,
+             int pass_index, const AdjStage* __restrict__ stages, const AdjStageOp* __restrict__ ops,
+             const int32_t* __restrict__ lslots, uint64_t tiles, double* __restrict__ partial)
+{
+    extern __shared__ __align__(16) double2 as_sm[];
+    __shared__ AdjTilePass P;
+    constexpr int WARPS = AS_THREADS / 32;
+    constexpr uint32_t T = 1u << AT_M;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(passes + pass_index);
+        uint4* dst = reinterpret_cast<uint4*>(&P);
+        for (int w = tid; w < (int)(sizeof(AdjTilePass) / 16); w += AS_THREADS) dst[w] = src[w];
+        __syncthreads();
+    }
+    double2* sp = as_sm;
+    double2* sl = as_sm + T;
+    double* wsum = reinterpret_cast<double*>(as_sm + 2 * T);      // [local slot][warp]
+    for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        uint64_t base = 0;
+        for (int j = 0; j < P.n_nonlocal; j++) base |= ((tile >> j) & 1ull) << P.nonlocal_q[j];
+        for (uint32_t l = tid; l < T; l += AS_THREADS) {
+            const uint64_t g = base + P.g_lo[l & 63u] + P.g_hi[l >> 6];
+            sp[l] = psi[g];
+            sl[l] = lam[g];
+        }
+        __syncthreads();
+        for (int st = P.stage_begin; st < P.stage_end; st++) {
+            const AdjStage S = stages[st];
+            uint32_t tb = 0;
+#pragma unroll
+            for (int b = 0; b < 7; b++) tb |= (uint32_t)((tid >> b) & 1) << S.tp[b];
+            const uint32_t o0 = 1u << S.rp[0], o1 = 1u << S.rp[1], o2 = 1u << S.rp[2];
+            double2 vp[AS_R], vl[AS_R];
+#pragma unroll
+            for (int r = 0; r < AS_R; r++) {
+                const uint32_t l = tb | ((r & 1) ? o0 : 0u) | ((r & 2) ? o1 : 0u) | ((r & 4) ? o2 : 0u);
+                vp[r] = sp[l];
+                vl[r] = sl[l];
+            }
+            for (int o = S.op_begin; o < S.op_end; o++) {
+                const AdjStageOp& op = ops[o];
+                const uint4 hdr = __ldg(reinterpret_cast<const uint4*>(&op));
+                const int kind = hdr.x & 0xFFu, j = (hdr.x >> 8) & 0xFFu, c = (hdr.x >> 16) & 0xFFu;
+                const int loc = hdr.x >> 24, nd = hdr.y & 0xFFu, lslot = (int)hdr.z;
+                Coef<double> inv;
+                {
+                    const double2* m2 = reinterpret_cast<const double2*>(op.m);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const double2 v = __ldg(m2 + q);
+                        inv.m[2 * q] = v.x;
+                        inv.m[2 * q + 1] = v.y;
+                    }
+                }
+                if (kind == AT_C1) {
+                    double dm[3][8];
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {
+                        const double2* m2 = reinterpret_cast<const double2*>(op.dm[d]);
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            const double2 v = d < nd ? __ldg(m2 + q) : make_double2(0.0, 0.0);
+                            dm[d][2 * q] = v.x;
+                            dm[d][2 * q + 1] = v.y;
+                        }
+                    }
+                    double acc[3] = {0.0, 0.0, 0.0};
+                    if (j == 0) as_c1<0>(vp, vl, inv, dm, nd, acc);
+                    else if (j == 1) as_c1<1>(vp, vl, inv, dm, nd, acc);
+                    else as_c1<2>(vp, vl, inv, dm, nd, acc);
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {
+                        if (d >= nd) break;
+                        double v = acc[d];
+#pragma unroll
+                        for (int sh = 16; sh > 0; sh >>= 1) v += __shfl_xor_sync(0xffffffffu, v, sh);
+                        if (lane == 0) wsum[(lslot + d) * WARPS + warp] = v;
+                    }
+                } else if (kind == AT_CX) {
+                    if (loc == AS_LOC_REG) {
+                        if (j == 0) { if (c == 1) as_swap_ctrl<0, 1>(vp, vl); else as_swap_ctrl<0, 2>(vp, vl); }
+                        else if (j == 1) { if (c == 0) as_swap_ctrl<1, 0>(vp, vl); else as_swap_ctrl<1, 2>(vp, vl); }
+                        else { if (c == 0) as_swap_ctrl<2, 0>(vp, vl); else as_swap_ctrl<2, 1>(vp, vl); }
+                    } else {
+                        const bool on = loc == AS_LOC_THREAD ? ((tid >> c) & 1) : ((tile >> c) & 1ull);
+                        if (on) {
+                            if (j == 0) as_swap_all<0>(vp, vl);
+                            else if (j == 1) as_swap_all<1>(vp, vl);
+                            else as_swap_all<2>(vp, vl);
+                        }
+                    }
+                } else {                     // AT_DIAG
+                    if (loc == AS_LOC_REG) {
+                        if (j == 0) as_diag_reg<0>(vp, vl, inv);
+                        else if (j == 1) as_diag_reg<1>(vp, vl, inv);
+                        else as_diag_reg<2>(vp, vl, inv);
+                    } else {
+                        const bool one = loc == AS_LOC_THREAD ? ((tid >> j) & 1) : ((tile >> j) & 1ull);
+#pragma unroll
+                        for (int r = 0; r < AS_R; r++) {
+                            if (one) {
+                                diag_one<double>(F_DIAG, inv, vp[r]);
+                                diag_one<double>(F_DIAG, inv, vl[r]);
+                            } else {
+                                diag_zero<double>(F_DIAG, inv, vp[r]);
+                                diag_zero<double>(F_DIAG, inv, vl[r]);
+                            }
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < AS_R; r++) {
+                const uint32_t l = tb | ((r & 1) ? o0 : 0u) | ((r & 2) ? o1 : 0u) | ((r & 4) ? o2 : 0u);
+                sp[l] = vp[r];
+                sl[l] = vl[r];
+            }
+            __syncthreads();
+        }
+        for (uint32_t l = tid; l < T; l += AS_THREADS) {
+            const uint64_t g = base + P.g_lo[l & 63u] + P.g_hi[l >> 6];
+            psi[g] = sp[l];
+            lam[g] = sl[l];
+        }
+        // the tile's derivative sums, warps added in a fixed order (the barrier after the
+        // last stage made every warp's sums visible)
+        for (int q = tid; q < P.n_lslots; q += AS_THREADS) {
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < WARPS; w++) v += wsum[q * WARPS + w];
+            partial[(uint64_t)lslots[P.lslot_begin + q] * tiles + tile] = v;
         }
         __syncthreads();
     }
@@ -419,6 +667,70 @@ bool append_pair_plan(PairPlan& all, const PairPlan& seg)
 }
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Groups each pass's ops into register stages for k_adj_stages (passes of AT_M local
+// qubits): ops are taken in order while their dense or CX targets fit 3 register
+// positions; the stage's other 7 local positions are the thread-index bits.
+void build_stages(std::vector<AdjTilePass>& tpasses, const std::vector<AdjTileOp>& tops,
+                  std::vector<AdjStage>& stages, std::vector<AdjStageOp>& sops)
+{
+    for (AdjTilePass& P : tpasses) {
+        P.stage_begin = (int32_t)stages.size();
+        int32_t o = P.op_begin;
+        while (o < P.op_end) {
+            std::vector<int> rp;
+            int32_t e = o;
+            for (; e < P.op_end; e++) {
+                const AdjTileOp& t = tops[e];
+                if (t.kind != AT_C1 && t.kind != AT_CX) continue;
+                if (std::find(rp.begin(), rp.end(), (int)t.p) != rp.end()) continue;
+                if (rp.size() == 3) break;
+                rp.push_back(t.p);
+            }
+            for (int q = 0; rp.size() < 3; q++)
+                if (std::find(rp.begin(), rp.end(), q) == rp.end()) rp.push_back(q);
+            AdjStage S;
+            std::memset(&S, 0, sizeof(S));
+            int nt = 0;
+            for (int j = 0; j < 3; j++) S.rp[j] = (uint8_t)rp[j];
+            for (int q = 0; q < AT_M; q++)
+                if (std::find(rp.begin(), rp.end(), q) == rp.end()) S.tp[nt++] = (uint8_t)q;
+            auto where = [&](int q, uint8_t& loc, uint8_t& bit) {
+                for (int j = 0; j < 3; j++)
+                    if (S.rp[j] == q) { loc = AS_LOC_REG; bit = (uint8_t)j; return; }
+                for (int b = 0; b < 7; b++)
+                    if (S.tp[b] == q) { loc = AS_LOC_THREAD; bit = (uint8_t)b; return; }
+            };
+            S.op_begin = (int32_t)sops.size();
+            for (int32_t k = o; k < e; k++) {
+                const AdjTileOp& t = tops[k];
+                AdjStageOp so;
+                std::memset(&so, 0, sizeof(so));
+                so.kind = t.kind;
+                so.nd = t.nd;
+                so.lslot = t.lslot;
+                std::memcpy(so.m, t.m, sizeof(so.m));
+                std::memcpy(so.dm, t.dm, sizeof(so.dm));
+                uint8_t loc = AS_LOC_REG;
+                if (t.kind == AT_C1) {
+                    where(t.p, loc, so.j);
+                } else if (t.kind == AT_CX) {
+                    where(t.p, loc, so.j);
+                    if (t.flags & 2) { so.loc = AS_LOC_TILE; so.c = t.tile_bit; }
+                    else where(t.c, so.loc, so.c);
+                } else {
+                    if (t.flags & 1) { so.loc = AS_LOC_TILE; so.j = t.tile_bit; }
+                    else where(t.p, so.loc, so.j);
+                }
+                sops.push_back(so);
+            }
+            S.op_end = (int32_t)sops.size();
+            stages.push_back(S);
+            o = e;
+        }
+        P.stage_end = (int32_t)stages.size();
+    }
+}
 
 }  // namespace
 }  // namespace svb
@@ -726,6 +1038,14 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
             if (ck < 0) break;
         }
     }
+    // register stages of the reverse passes (tiles of AT_M qubits)
+    const bool staged_rev = TM == AT_M;
+    std::vector<AdjStage> stages;
+    std::vector<AdjStageOp> sops;
+    if (staged_rev) build_stages(tpasses, tops, stages, sops);
+    if ((err = grow(A.rev_stages, std::max<size_t>(1, stages.size()) * sizeof(AdjStage))) != cudaSuccess ||
+        (err = grow(A.rev_sops, std::max<size_t>(1, sops.size()) * sizeof(AdjStageOp))) != cudaSuccess)
+        return fail(err, "cudaMalloc(reverse plan)");
     if ((err = grow(A.rev_passes, std::max<size_t>(1, tpasses.size()) * sizeof(AdjTilePass))) != cudaSuccess)
         return fail(err, "cudaMalloc(reverse plan)");
     if ((err = grow(A.rev_ops, std::max<size_t>(1, tops.size()) * sizeof(AdjTileOp))) != cudaSuccess)
@@ -737,7 +1057,9 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
     // results come back into the stage's tail
     const size_t rev_bytes = align_up(tslots.size() * sizeof(int32_t)) +
                              align_up(tpasses.size() * sizeof(AdjTilePass)) +
-                             align_up(tops.size() * sizeof(AdjTileOp));
+                             (staged_rev ? align_up(stages.size() * sizeof(AdjStage)) +
+                                               align_up(sops.size() * sizeof(AdjStageOp))
+                                         : align_up(tops.size() * sizeof(AdjTileOp)));
     const size_t res_bytes = (slots.size() + 1) * sizeof(double);
     if (A.host_stage.cap < fwd_bytes + rev_bytes + res_bytes) {
         // growing would free memory the forward copies may still read: wait for them
@@ -756,11 +1078,42 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
         };
         stage(tslots.data(), tslots.size() * sizeof(int32_t), A.rev_slots.p);
         stage(tpasses.data(), tpasses.size() * sizeof(AdjTilePass), A.rev_passes.p);
-        stage(tops.data(), tops.size() * sizeof(AdjTileOp), A.rev_ops.p);
+        if (staged_rev) {
+            stage(stages.data(), stages.size() * sizeof(AdjStage), A.rev_stages.p);
+            stage(sops.data(), sops.size() * sizeof(AdjStageOp), A.rev_sops.p);
+        } else {
+            stage(tops.data(), tops.size() * sizeof(AdjTileOp), A.rev_ops.p);
+        }
         if (err != cudaSuccess) return fail(err, "reverse plan upload");
     }
     double2* psi = static_cast<double2*>(s->state);
-    {
+    if (staged_rev) {
+        static int ctas_per_sm = 0, sms = 0;
+        const size_t smem = (2 * sizeof(double2) << AT_M) + AT_MAX_LSLOTS * (AS_THREADS / 32) * sizeof(double);
+        if (ctas_per_sm == 0) {
+            if ((err = cudaFuncSetAttribute(k_adj_stages, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+                    cudaSuccess ||
+                (err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, k_adj_stages, AS_THREADS, smem)) !=
+                    cudaSuccess ||
+                (err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device)) != cudaSuccess)
+                return fail(err, "reverse kernel setup");
+            ctas_per_sm = std::max(ctas_per_sm, 1);
+        }
+        const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)ctas_per_sm * sms);
+        const size_t dyn = (2 * sizeof(double2) << AT_M) + (size_t)max_lslots * (AS_THREADS / 32) * sizeof(double);
+        size_t pi = 0;
+        for (const Seg& sg : segs) {
+            for (; pi < sg.pass_end; pi++)
+                k_adj_stages<<<grid, AS_THREADS, dyn>>>(psi, lam, static_cast<const AdjTilePass*>(A.rev_passes.p),
+                                                        (int)pi, static_cast<const AdjStage*>(A.rev_stages.p),
+                                                        static_cast<const AdjStageOp*>(A.rev_sops.p),
+                                                        static_cast<const int32_t*>(A.rev_slots.p), tiles, partial);
+            if ((err = cudaGetLastError()) != cudaSuccess) return fail(err, "reverse pass");
+            if (sg.ck >= 0 &&
+                (err = cudaMemcpyAsync(psi, ckpts[sg.ck], sbytes, cudaMemcpyDeviceToDevice)) != cudaSuccess)
+                return fail(err, "checkpoint reload");
+        }
+    } else {
         static int ctas_per_sm = 0, sms = 0;
         // the tiles and the warps' sums of up to AT_MAX_LSLOTS slots of a pass
         const size_t smem = (2 * sizeof(double2) << AT_M) + AT_MAX_LSLOTS * (AT_THREADS / 32) * sizeof(double);

@@ -253,6 +253,8 @@ void free_adjoint_scratch(AdjScratch& a)
     release(a.rev_passes);
     release(a.rev_ops);
     release(a.rev_slots);
+    release(a.rev_stages);
+    release(a.rev_sops);
     release_host(a.host_stage);
     for (GrowBuf& b : a.ckpts) release(b);
     a.ckpts.clear();

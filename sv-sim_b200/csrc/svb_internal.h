@@ -416,6 +416,7 @@ struct AdjScratch {
     GrowBuf plan_passes, plan_stages, plan_ops;     // forward segments' staged plans
     GrowBuf pair_passes, pair_ops, pair_layouts, pair_gates;   // or their pair plans
     GrowBuf rev_passes, rev_ops, rev_slots;         // the tiled reverse sweep's plan
+    GrowBuf rev_stages, rev_sops;                   // its register stages (tiles of 10 qubits)
     std::vector<GrowBuf> ckpts;
 };
 
