@@ -63,7 +63,7 @@ def parse():
                     help="headline: the FP64 n=30 step (the measured line); the others run one "
                          "secondary form alone (for profiling and capacity runs)")
     ap.add_argument("--instances", type=int, default=512, help="QAOA batch size (--form qaoa)")
-    ap.add_argument("--fusion-width", type=int, default=FUSION_WIDTH, choices=[3, 4, 5],
+    ap.add_argument("--fusion-width", type=int, default=FUSION_WIDTH, choices=[3, 4, 5, 6],
                     help="qubits per fused block of the tensor-core FP32 form")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="state precision of --form qaoa")
@@ -913,7 +913,7 @@ def secondary_forms(device, circuit):
     forms = {}
     forms["per_gate_fp64"] = per_gate_form(device, circuit)
     forms["config1_n16_brickwork"] = config1_form(device)
-    for k in (4, 5):
+    for k in (4, 5, 6):
         forms[f"fused_tc_fp32_k{k}"] = fused_form(device, circuit, k=k)
     forms["qaoa_batch_fp64"] = qaoa_form(device, 512, "fp64")
     forms["qaoa_batch_fp32"] = qaoa_form(device, 512, "fp32")

@@ -121,8 +121,8 @@ svb_status svb_set_circuit(svb_sim* sim, const svb_gate* gates, size_t n_gates);
 svb_status svb_clear_circuit(svb_sim* sim);
 
 /* Chooses the execution engine (svb_engine) for the next svb_set_circuit; tile_bits
- * (0 = automatic) and fusion_width (0 = automatic, else 2..6) tune the staged and
- * fused engines. */
+ * (0 = automatic) and fusion_width (0 = automatic: 5; else 3..6, where 6 runs one block
+ * per pass) tune the staged and fused engines. */
 svb_status svb_set_engine(svb_sim* sim, int engine, int tile_bits, int fusion_width);
 
 /* Result of svb_autotune. */
@@ -139,7 +139,7 @@ typedef struct svb_tune_result {
 /* Autotuner (no reference counterpart; the reference fixes its launch shape,
  * svsim_nvgpu_sin.cuh:309-316, config.hpp:48): times every engine configuration that can
  * run the circuit on this handle (per-gate for n <= 26; staged at each tile size; the pair
- * engine for FP64 or the fused engine at k = 3..5 for FP32, when the circuit has no SRN)
+ * engine for FP64 or the fused engine at k = 3..6 for FP32, when the circuit has no SRN)
  * on its first min(n_gates, 360) gates, one warm-up and one timed run each, and keeps the
  * fastest for this circuit structure (qubit count, precision, and the ops and qubits of
  * every elementary op; angles ignored): from then on svb_set_circuit with

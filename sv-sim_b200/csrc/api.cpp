@@ -70,6 +70,7 @@ void free_plan(Sim* s)
     s->staged = StagedPlan{};
     cudaFree(s->dfused.passes);
     cudaFree(s->dfused.blocks);
+    cudaFree(s->dfused.passes6);
     cudaFree(s->dfused.gates);
     cudaFree(s->dfused.err);
     cudaFree(s->dfused.norm_partial);
@@ -149,12 +150,19 @@ svb_status launch_all(Sim* s, cudaStream_t st)
     const int n = (int)s->n;
     if (s->engine == SVB_ENGINE_FUSED) {
         const FusedPlan& F = s->fused;
-        for (size_t p = 0; p < F.passes.size(); p++) {
-            cudaError_t e = launch_fused_pass(s->state, n, F.k, (int)p, F.passes[p].n_blocks, 0,
-                                              s->dfused, st);
-            if (e != cudaSuccess) return cuda_fail(e, "fused pass launch");
+        if (F.k == F6_K) {
+            for (size_t p = 0; p < F.passes6.size(); p++) {
+                cudaError_t e = launch_fused6_pass(s->state, n, (int)p, s->dfused, st);
+                if (e != cudaSuccess) return cuda_fail(e, "fused pass launch");
+            }
+        } else {
+            for (size_t p = 0; p < F.passes.size(); p++) {
+                cudaError_t e = launch_fused_pass(s->state, n, F.k, (int)p, F.passes[p].n_blocks, 0,
+                                                  s->dfused, st);
+                if (e != cudaSuccess) return cuda_fail(e, "fused pass launch");
+            }
         }
-        if (!F.passes.empty()) {
+        if (F.n_passes() > 0) {
             cudaError_t e = launch_fused_renorm(s->state, n, s->dfused, st);
             if (e != cudaSuccess) return cuda_fail(e, "fused renormalisation");
         }
@@ -449,7 +457,7 @@ svb_status svb_set_engine(svb_sim* s, int engine, int tile_bits, int fusion_widt
     if (tile_bits != 0 && !staged_supported(s->precision, tile_bits))
         return invalid("svb_set_engine: tile_bits must be 10..12 (FP64) or 11..13 (FP32)");
     if (fusion_width != 0 && (fusion_width < FT_MIN_K || fusion_width > FT_MAX_K))
-        return invalid("svb_set_engine: fusion_width must be 3..5");
+        return invalid("svb_set_engine: fusion_width must be 3..6");
     s->engine_req = engine;
     s->tile_bits_req = tile_bits;
     s->fusion_req = fusion_width;
@@ -569,8 +577,9 @@ svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* g
     s->info.model_bytes = 2.0 * sb * sweeps;
     s->info.engine = engine;
     if (engine == SVB_ENGINE_FUSED) {
-        const int k = fusion ? fusion : FT_MAX_K;
-        plan_fused(s->eops, n, k, s->fused);
+        const int k = fusion ? fusion : FT_DEFAULT_K;
+        if (k == F6_K) plan_fused6(s->eops, n, s->fused);
+        else plan_fused(s->eops, n, k, s->fused);
         const FusedPlan& F = s->fused;
         SVB_CUDA(cudaMalloc(&s->dfused.passes, std::max<size_t>(1, F.passes.size()) * sizeof(FusedPass)),
                  "cudaMalloc(plan)");
@@ -590,13 +599,19 @@ svb_status set_circuit_lowered(Sim* s, std::vector<EOp>& eops, const svb_gate* g
         if (!F.gates.empty())
             SVB_CUDA(cudaMemcpy(s->dfused.gates, F.gates.data(), F.gates.size() * sizeof(float),
                                 cudaMemcpyHostToDevice), "plan upload");
-        s->info.n_passes = F.passes.size();
-        s->info.tile_bits = FT_TILE_BITS;
-        s->info.n_blocks = F.blocks.size();
+        if (!F.passes6.empty()) {
+            SVB_CUDA(cudaMalloc(&s->dfused.passes6, F.passes6.size() * sizeof(Fused6Pass)), "cudaMalloc(plan)");
+            SVB_CUDA(cudaMemcpy(s->dfused.passes6, F.passes6.data(), F.passes6.size() * sizeof(Fused6Pass),
+                                cudaMemcpyHostToDevice), "plan upload");
+        }
+        const size_t np = F.n_passes();
+        s->info.n_passes = np;
+        s->info.tile_bits = k == F6_K ? F6_TILE_BITS : FT_TILE_BITS;
+        s->info.n_blocks = k == F6_K ? F.passes6.size() : F.blocks.size();
         s->info.plan_bytes = F.passes.size() * sizeof(FusedPass) + F.blocks.size() * sizeof(FusedBlock) +
-                             F.gates.size() * sizeof(float);
+                             F.passes6.size() * sizeof(Fused6Pass) + F.gates.size() * sizeof(float);
         // one read + write per pass, then the renormalisation (two reads, one write)
-        s->info.moved_bytes = 2.0 * sb * (double)F.passes.size() + (F.passes.empty() ? 0.0 : 3.0 * sb);
+        s->info.moved_bytes = 2.0 * sb * (double)np + (np == 0 ? 0.0 : 3.0 * sb);
     } else if (engine == SVB_ENGINE_PAIRS) {
         if (!plan_pairs(s->eops, n, s->pairs, &s->mats)) {
             set_error("svb_set_circuit: the pair planner rejected the circuit");

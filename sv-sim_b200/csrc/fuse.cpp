@@ -360,4 +360,196 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
     }
 }
 
+namespace {
+
+// U[r][c] (row-major, 2^|tq| square) of the ops in `idx` on the qubits tq (bit i of the
+// matrix index <-> qubit tq[i]), multiplied out in FP64 column by column
+void block_unitary(const std::vector<EOp>& ops, const std::vector<int>& idx, const std::vector<int>& tq,
+                   std::vector<cplx>& U)
+{
+    int pos_of[64];
+    for (int q = 0; q < 64; q++) pos_of[q] = -1;
+    for (size_t i = 0; i < tq.size(); i++) pos_of[tq[i]] = (int)i;
+    const int d = 1 << (int)tq.size();
+    U.assign((size_t)d * d, cplx(0, 0));
+    std::vector<cplx> col(d);
+    for (int c = 0; c < d; c++) {
+        std::fill(col.begin(), col.end(), cplx(0, 0));
+        col[c] = 1.0;
+        for (int i : idx) apply_small(ops[i], pos_of, col);
+        for (int r = 0; r < d; r++) U[(size_t)r * d + c] = col[r];
+    }
+}
+
+}  // namespace
+
+// Fusion width 6: the op stream is cut greedily into blocks of at most 6 qubits (an op
+// joins the current block when it touches no qubit of an op left out before it and the
+// union stays within 6 qubits; ops on disjoint qubits commute, so later ops may be pulled
+// forward past those left out).  Each block is one pass over tiles of 4,096 amplitudes:
+// its 6 target qubits (padded with high qubits when it has fewer) and the 6 lowest other
+// qubits as row bits, so a tile always holds qubits 0 and 1 (whole 32-byte sectors).
+//
+// The kernel (kernels_fused6.cu) moves amplitude x = thread + 512 i (i < 8) of a tile;
+// the planner maps the 12 bits of x onto local qubits so that the 16 threads of a half
+// warp hit 16 distinct bank pairs of the B-operand plane: x bits 0 and 1 are qubits 0 and
+// 1 (the two lowest local qubits), and x bits 2 and 3 are chosen to complete the four
+// low word-offset bits, which come from target bit 0 (+1 word) and row bits 0..2 (+2, +4,
+// +8 words) of the canonical K-major layout.  When qubits 0 and 1 are both targets two
+// of the half warp's words share a bank pair (a 2-way conflict).
+void plan_fused6(const std::vector<EOp>& ops, int n, FusedPlan& plan)
+{
+    plan = FusedPlan{};
+    plan.k = F6_K;
+    const size_t N_ops = ops.size();
+    const uint64_t all = (n >= 64) ? ~0ull : (bit(n) - 1);
+    std::vector<char> done(N_ops, 0);
+    size_t first = 0;
+    std::vector<int> blk;
+    std::vector<cplx> U;
+    for (;;) {
+        while (first < N_ops && done[first]) first++;
+        if (first == N_ops) break;
+        uint64_t S = 0, blocked = 0;
+        blk.clear();
+        for (size_t i = first; i < N_ops; i++) {
+            if (done[i]) continue;
+            const uint64_t t = op_qubits(ops[i]);
+            if ((t & blocked) || __builtin_popcountll(S | t) > F6_K) {
+                blocked |= t;
+                if (blocked == all) break;
+                continue;
+            }
+            S |= t;
+            blk.push_back((int)i);
+            done[i] = 1;
+        }
+        // targets: the block's qubits, padded from the top; rows: the 6 lowest others
+        uint64_t T = S;
+        for (int q = n - 1; q >= 0 && __builtin_popcountll(T) < F6_K; q--) T |= bit(q);
+        uint64_t R = 0;
+        for (int q = 0; q < n && __builtin_popcountll(R) < F6_TILE_BITS - F6_K; q++)
+            if (!((T >> q) & 1)) R |= bit(q);
+        const uint64_t L = T | R;
+
+        Fused6Pass P;
+        std::memset(&P, 0, sizeof(P));
+        int nl = 0, nn = 0;
+        for (int q = 0; q < n; q++) {
+            if ((L >> q) & 1) P.local_q[nl++] = (uint8_t)q;
+            else P.nonlocal_q[nn++] = (uint8_t)q;
+        }
+        P.n_nonlocal = nn;
+
+        // roles: target bit order tq (bit i of a <-> tq[i]) and row bit order rq
+        std::vector<int> tq, rq;
+        const int q0 = P.local_q[0], q1 = P.local_q[1];
+        const bool t0 = (T >> q0) & 1, t1 = (T >> q1) & 1;
+        int xq2 = -1, xq3 = -1;            // the qubits of x bits 2 and 3
+        auto first_of = [&](uint64_t set, uint64_t skip) {
+            for (int i = 2; i < F6_TILE_BITS; i++) {
+                const int q = P.local_q[i];
+                if (((set >> q) & 1) && !((skip >> q) & 1)) return q;
+            }
+            return -1;
+        };
+        if (!t0 && !t1) {                  // rows 0, 1 <- q0, q1; x2 -> target bit 0, x3 -> row 2
+            rq = {q0, q1};
+            xq2 = first_of(T, 0);
+            xq3 = first_of(R, 0);
+            tq = {xq2};
+            rq.push_back(xq3);
+        } else if (t0 != t1) {             // target bit 0 and row 0 <- q0, q1; x2, x3 -> rows 1, 2
+            const int qt = t0 ? q0 : q1, qr = t0 ? q1 : q0;
+            tq = {qt};
+            rq = {qr};
+            xq2 = first_of(R, 0);
+            xq3 = first_of(R, bit(xq2));
+            rq.push_back(xq2);
+            rq.push_back(xq3);
+        } else {                           // both targets: 2-way; x2, x3 -> rows 0, 1
+            tq = {q0, q1};
+            xq2 = first_of(R, 0);
+            xq3 = first_of(R, bit(xq2));
+            rq = {xq2, xq3};
+        }
+        for (int i = 0; i < F6_TILE_BITS; i++) {
+            const int q = P.local_q[i];
+            const bool in_t = std::find(tq.begin(), tq.end(), q) != tq.end();
+            const bool in_r = std::find(rq.begin(), rq.end(), q) != rq.end();
+            if (in_t || in_r) continue;
+            if ((T >> q) & 1) tq.push_back(q);
+            else rq.push_back(q);
+        }
+        // x bits -> qubits: 0, 1 -> q0, q1; 2, 3 -> xq2, xq3; the rest ascending
+        int xq[F6_TILE_BITS];
+        xq[0] = q0;
+        xq[1] = q1;
+        xq[2] = xq2;
+        xq[3] = xq3;
+        for (int i = 2, j = 4; i < F6_TILE_BITS; i++) {
+            const int q = P.local_q[i];
+            if (q != xq2 && q != xq3) xq[j++] = q;
+        }
+        // word offset of a qubit's bit in the B-operand plane: target bit b -> 1 (b = 0)
+        // or 128 << (b - 1); row bit b -> 2 << b
+        auto word_of = [&](int q) -> uint32_t {
+            for (int b = 0; b < F6_K; b++)
+                if (tq[b] == q) return b == 0 ? 1u : (128u << (b - 1));
+            for (int b = 0; b < F6_TILE_BITS - F6_K; b++)
+                if (rq[b] == q) return 2u << b;
+            return 0u;
+        };
+        for (int j = 0; j < 64; j++) {
+            uint64_t glo = 0, ghi = 0;
+            uint32_t slo = 0, shi = 0;
+            for (int b = 0; b < 6; b++) {
+                if ((j >> b) & 1) {
+                    glo |= bit(xq[b]);
+                    ghi |= bit(xq[6 + b]);
+                    slo += word_of(xq[b]);
+                    shi += word_of(xq[6 + b]);
+                }
+            }
+            P.g_lo[j] = glo;
+            P.g_hi[j] = ghi;
+            P.s_lo[j] = (uint16_t)slo;
+            P.s_hi[j] = (uint16_t)shi;
+            uint64_t orow = 0, otgt = 0;
+            for (int b = 0; b < 6; b++) {
+                if ((j >> b) & 1) {
+                    orow |= bit(rq[b]);
+                    otgt |= bit(tq[b]);
+                }
+            }
+            P.o_row[j] = orow;
+            P.o_tgt[j] = otgt;
+        }
+        P.rows_paired = (P.o_row[1] == 1) ? 1 : 0;   // row bit 0 is qubit 0
+
+        // the real form G[m'][kk] (m' = 2a' + c', kk = 2a + c) of the block's matrix,
+        // row-major, hi plane then lo plane (both rounded to nearest TF32)
+        block_unitary(ops, blk, tq, U);
+        P.gate_word = (uint32_t)plan.gates.size();
+        plan.gates.resize(plan.gates.size() + 2 * (size_t)F6_N * F6_N);
+        float* gh = plan.gates.data() + P.gate_word;
+        float* gl = gh + (size_t)F6_N * F6_N;
+        const int d = 1 << F6_K;
+        for (int mp = 0; mp < F6_N; mp++) {
+            const int ar = mp >> 1, cr = mp & 1;
+            for (int kk = 0; kk < F6_N; kk++) {
+                const int ac = kk >> 1, cc = kk & 1;
+                const cplx u = U[(size_t)ar * d + ac];
+                double val;
+                if (cr == 0) val = cc == 0 ? u.real() : -u.imag();
+                else val = cc == 0 ? u.imag() : u.real();
+                const float h = tf32_hi((float)val);
+                gh[(size_t)mp * F6_N + kk] = h;
+                gl[(size_t)mp * F6_N + kk] = tf32_hi((float)(val - (double)h));
+            }
+        }
+        plan.passes6.push_back(P);
+    }
+}
+
 }  // namespace svb

@@ -233,7 +233,8 @@ __host__ __device__ constexpr int fused_raw_buffers(int k) { return k >= 5 ? 1 :
 constexpr int FT_EPI_WARPS = 16;     // warps that move tiles and operands: four per TMEM lane quadrant
 constexpr int FT_THREADS = 32 * (FT_EPI_WARPS + 1);   // plus one warp that issues the MMAs
 constexpr int FT_MAX_NONLOCAL = 24;  // tile-index bits of a pass (n <= 36)
-constexpr int FT_MIN_K = 3, FT_MAX_K = 5;
+constexpr int FT_MIN_K = 3, FT_MAX_K = 6;   // 6: one block per pass (kernels_fused6.cu)
+constexpr int FT_DEFAULT_K = 5;          // the fastest width on the random circuits measured
 
 // Shared-memory layouts of the fused kernel.  All are linear over GF(2) in the bits they
 // index, so tables of them combine by XOR.
@@ -291,25 +292,64 @@ struct FusedPass {
 };
 static_assert(sizeof(FusedPass) % 16 == 0, "FusedPass layout");
 
+// Fusion width 6 (kernels_fused6.cu): one 6-qubit block per pass, applied in the
+// transposed form D^T = G X^T.  The block's real form G (128 x 128: M = 128 rows, the full
+// width of one tcgen05.mma) is the A operand and stays in tensor memory for the whole
+// launch; the state tile (4,096 amplitudes: the 6 target qubits and the 6 lowest other
+// qubits) is the B operand in shared memory, where the loaded FP32 values themselves are
+// the hi plane.  A pass is one block: two 6-qubit blocks' hi + lo operands (256 KiB) do
+// not fit on one SM.
+constexpr int F6_K = 6;
+constexpr int F6_TILE_BITS = 12;     // 6 target + 6 row bits: 64 rows of 64 amplitudes
+constexpr int F6_ROWS = 64;          // N of the MMA: rows of the tile
+constexpr int F6_N = 128;            // real dimension 2^(k+1): M and K of the MMA
+constexpr int F6_SLOTS = 3;          // tiles in flight (shared memory: hi + lo plane each)
+
+struct Fused6Pass {                  // one 6-qubit block = one pass
+    uint8_t local_q[F6_TILE_BITS];   // the tile's qubits, ascending
+    uint8_t nonlocal_q[64 - F6_TILE_BITS];   // tile index bit j <-> nonlocal_q[j]
+    // The kernel moves amplitude x = thread + 512 i of a tile (12 bits, mapped onto the
+    // local qubits by the planner): its global offset g_lo[x & 63] | g_hi[x >> 6] and its
+    // word (8-byte) offset s_lo[x & 63] + s_hi[x >> 6] in a B-operand plane (canonical
+    // K-major layout without swizzle, 64 rows: target bit 0 -> 1 word, target bit b > 0
+    // -> 128 << (b - 1), row bit b -> 2 << b)
+    uint64_t g_lo[64];
+    uint64_t g_hi[64];
+    uint16_t s_lo[64];
+    uint16_t s_hi[64];
+    uint64_t o_row[64];              // row index n -> global amplitude offset of its bits
+    uint64_t o_tgt[64];              // target index a -> global amplitude offset of its bits
+    uint32_t gate_word;              // float offset of G_hi (row-major 128 x 128), G_lo after it
+    int32_t n_nonlocal;
+    int32_t rows_paired;             // 1 when row bit 0 is qubit 0 (rows 2r, 2r+1 adjacent)
+    int32_t pad;
+};
+static_assert(sizeof(Fused6Pass) % 16 == 0, "Fused6Pass layout");
+
 struct FusedPlan {
     int k = 0;
     std::vector<FusedPass> passes;
     std::vector<FusedBlock> blocks;
+    std::vector<Fused6Pass> passes6; // fusion width 6: one block per pass
     std::vector<float> gates;        // per block: hi plane then lo plane, canonical layout
+    size_t n_passes() const { return k == F6_K ? passes6.size() : passes.size(); }
 };
 
 bool fusable(const std::vector<EOp>& ops);
 void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan);
+void plan_fused6(const std::vector<EOp>& ops, int n, FusedPlan& plan);
 
 struct DevFusedBuffers {
     FusedPass* passes = nullptr;
     FusedBlock* blocks = nullptr;
+    Fused6Pass* passes6 = nullptr;
     float* gates = nullptr;
     int* err = nullptr;
     double* norm_partial = nullptr;      // REDUCE_BLOCKS FP64 partial sums of |a|^2
 };
 cudaError_t launch_fused_pass(void* state, int n, int k, int pass_index, int n_blocks,
                               int gate_words_per_block, const DevFusedBuffers& b, cudaStream_t s);
+cudaError_t launch_fused6_pass(void* state, int n, int pass_index, const DevFusedBuffers& b, cudaStream_t s);
 // Rescales the FP32 state to unit norm (norm summed in FP64) after a fused run.
 cudaError_t launch_fused_renorm(void* state, int n, const DevFusedBuffers& b, cudaStream_t s);
 

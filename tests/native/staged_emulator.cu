@@ -192,7 +192,7 @@ static uint32_t emu_kmajor(uint32_t row, uint32_t kk, uint32_t rows)
 extern "C" int emu_fused_run(uint32_t n, const svb_gate* gates, size_t n_gates, int k,
                              double* re, double* im, uint64_t* n_passes, uint64_t* n_blocks)
 {
-    if ((int)n < FT_TILE_BITS || k < FT_MIN_K || k > FT_MAX_K) return -1;
+    if ((int)n < FT_TILE_BITS || k < FT_MIN_K || k >= F6_K) return -1;
     std::vector<EOp> eops;
     for (size_t i = 0; i < n_gates; i++)
         if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
@@ -276,6 +276,64 @@ extern "C" int emu_fused_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
     return 0;
 }
 
+// Fusion width 6 (plan_fused6, kernels_fused6.cu): amplitude x = thread + 512 i of a tile
+// is copied to word s_lo[x & 63] + s_hi[x >> 6] of the B-operand plane (each word once);
+// the MMA reads X[n][kk] at the canonical K-major position of (row n, kk) among 64 rows;
+// D^T[m'][n] = sum_kk (G_hi + G_lo)[m'][kk] X[n][kk]; amplitude (n, a') of the output goes
+// to o_row[n] | o_tgt[a'] (each once), and pairs of rows share one 16-byte store when
+// rows_paired is set.  The arithmetic is FP64; only the layouts and tables are under test.
+extern "C" int emu_fused6_run(uint32_t n, const svb_gate* gates, size_t n_gates, double* re, double* im,
+                              uint64_t* n_passes)
+{
+    if ((int)n < F6_TILE_BITS) return -1;
+    std::vector<EOp> eops;
+    for (size_t i = 0; i < n_gates; i++)
+        if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
+    if (!fusable(eops)) return -3;
+    FusedPlan plan;
+    plan_fused6(eops, (int)n, plan);
+    if (n_passes) *n_passes = plan.passes6.size();
+    const uint64_t tiles = 1ull << (n - F6_TILE_BITS);
+    std::vector<double> plane(4096 * 2), D((size_t)F6_N * F6_ROWS);
+    for (const Fused6Pass& P : plan.passes6) {
+        if (P.n_nonlocal != (int)n - F6_TILE_BITS) return -5;
+        if (P.rows_paired)
+            for (int r = 0; r < F6_ROWS; r += 2)
+                if (P.o_row[r + 1] != P.o_row[r] + 1) return -6;
+        const float* gh = plan.gates.data() + P.gate_word;
+        const float* gl = gh + (size_t)F6_N * F6_N;
+        for (uint64_t t = 0; t < tiles; t++) {
+            uint64_t base = 0;
+            for (int j = 0; j < P.n_nonlocal; j++) base |= ((t >> j) & 1ull) << P.nonlocal_q[j];
+            std::vector<int> seen(4096, 0);
+            for (uint32_t x = 0; x < 4096; x++) {
+                const uint64_t g = base + (P.g_lo[x & 63] | P.g_hi[x >> 6]);
+                const uint32_t w = (uint32_t)P.s_lo[x & 63] + (uint32_t)P.s_hi[x >> 6];
+                if (w >= 4096 || seen[w]++) return -2;
+                plane[2 * w] = re[g];
+                plane[2 * w + 1] = im[g];
+            }
+            for (int nr = 0; nr < F6_ROWS; nr++)
+                for (int mp = 0; mp < F6_N; mp++) {
+                    double s = 0;
+                    for (int kk = 0; kk < F6_N; kk++)
+                        s += ((double)gh[(size_t)mp * F6_N + kk] + (double)gl[(size_t)mp * F6_N + kk]) *
+                             plane[emu_kmajor((uint32_t)nr, (uint32_t)kk, F6_ROWS)];
+                    D[(size_t)mp * F6_ROWS + nr] = s;
+                }
+            std::vector<int> out(4096, 0);
+            for (int nr = 0; nr < F6_ROWS; nr++)
+                for (int a = 0; a < (1 << F6_K); a++) {
+                    const uint64_t off = P.o_row[nr] | P.o_tgt[a];
+                    if (off >= (1ull << n) || (off & ~(P.g_lo[63] | P.g_hi[63])) != 0) return -4;
+                    re[base + off] = D[(size_t)(2 * a) * F6_ROWS + nr];
+                    im[base + off] = D[(size_t)(2 * a + 1) * F6_ROWS + nr];
+                }
+        }
+    }
+    return 0;
+}
+
 // passes and blocks of a fused plan, without running it
 extern "C" int emu_fused_stats(uint32_t n, const svb_gate* gates, size_t n_gates, int k, uint64_t* n_passes,
                                uint64_t* n_blocks)
@@ -286,9 +344,10 @@ extern "C" int emu_fused_stats(uint32_t n, const svb_gate* gates, size_t n_gates
         if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
     if (!fusable(eops)) return -3;
     FusedPlan plan;
-    plan_fused(eops, (int)n, k, plan);
-    *n_passes = plan.passes.size();
-    *n_blocks = plan.blocks.size();
+    if (k == F6_K) plan_fused6(eops, (int)n, plan);
+    else plan_fused(eops, (int)n, k, plan);
+    *n_passes = plan.n_passes();
+    *n_blocks = k == F6_K ? plan.passes6.size() : plan.blocks.size();
     return 0;
 }
 

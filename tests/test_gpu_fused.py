@@ -19,11 +19,12 @@ def run_fused(n, gates, k):
     return h
 
 
-@pytest.mark.parametrize("k", [3, 4, 5])
+@pytest.mark.parametrize("k", [3, 4, 5, 6])
 @pytest.mark.parametrize("n", [12, 14, 17, 22])
 def test_fused_matches_oracle(oracle, n, k):
     """n = 12..17 give each CTA one tile; n = 22 (1,024 tiles) gives each several, so both
-    tile slots, the prefetch buffers' reuse and the output stage's reuse run."""
+    tile slots (three at k = 6), the prefetch buffers' reuse and the output stage's reuse
+    run."""
     g = circuits.random_matching_circuit(n, 8, seed=100 * n + k)
     h = run_fused(n, g, k)
     re, im = h.get_state()
@@ -47,13 +48,14 @@ def test_fused_every_op(oracle):
                 "U1", "RX", "RY", "RZ", "CRX", "CRY", "CRZ", "CU1", "RXX", "RZZ", "RYY", "R") else 0)
             gl.append(G.FACTORIES[name](*([rng.uniform(-math.pi, math.pi) for _ in range(npar)] + qs)))
     g = G.to_array(gl)
-    h = run_fused(n, g, 4)
-    re, im = h.get_state()
     ore, oim = oracle.run(n, g)
-    assert 1 - fidelity(re + 1j * im, ore + 1j * oim) <= 1e-6
+    for k in (4, 6):
+        h = run_fused(n, g, k)
+        re, im = h.get_state()
+        assert 1 - fidelity(re + 1j * im, ore + 1j * oim) <= 1e-6, k
 
 
-@pytest.mark.parametrize("k", [4, 5])
+@pytest.mark.parametrize("k", [4, 5, 6])
 def test_fused_vs_fp64_on_device(k):
     from svsim_b200 import _native as nat
     n = 22
@@ -69,10 +71,13 @@ def test_fused_vs_fp64_on_device(k):
 def test_fused_rejects_srn_and_fp64():
     from svsim_b200 import _native as nat
     h = nat.Handle(12, 0, nat.SVB_FP32)
-    h.set_engine(nat.ENGINE_FUSED, 0, 4)
-    with pytest.raises(nat.SvbError) as e:
-        h.set_circuit(G.to_array([G.SRN(0)]))
-    assert e.value.status == nat.SVB_ERR_UNSUPPORTED
+    for k in (4, 6):
+        h.set_engine(nat.ENGINE_FUSED, 0, k)
+        with pytest.raises(nat.SvbError) as e:
+            h.set_circuit(G.to_array([G.SRN(0)]))
+        assert e.value.status == nat.SVB_ERR_UNSUPPORTED
+    with pytest.raises(nat.SvbError):
+        h.set_engine(nat.ENGINE_FUSED, 0, 7)
     h64 = nat.Handle(12, 0, nat.SVB_FP64)
     with pytest.raises(nat.SvbError):
         h64.set_engine(nat.ENGINE_FUSED, 0, 4)
@@ -85,14 +90,15 @@ def test_fused_run_keeps_unit_norm_and_small_amplitude_error():
     from svsim_b200 import _native as nat
     n = 20
     g = circuits.random_matching_circuit(n, 40, seed=9)
-    h32 = run_fused(n, g, 4)
-    assert abs(h32.norm2() - 1.0) <= 2e-6
     h64 = nat.Handle(n, 0, nat.SVB_FP64)
     h64.set_circuit(g)
     h64.run()
-    f, d = h64.compare(h32)
     amp = 2.0 ** (-n / 2)
-    assert 1 - f <= 1e-9 and d <= 2e-4 * amp, (1 - f, d)
+    for k in (4, 6):
+        h32 = run_fused(n, g, k)
+        assert abs(h32.norm2() - 1.0) <= 2e-6
+        f, d = h64.compare(h32)
+        assert 1 - f <= 1e-9 and d <= 2e-4 * amp, (k, 1 - f, d)
 
 
 def test_auto_engine_runs_fp32_circuits_on_the_fused_engine(oracle):

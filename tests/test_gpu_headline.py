@@ -151,7 +151,7 @@ def test_headline_fp64_matches_reference(golden, engine):
         h.close()
 
 
-@pytest.mark.parametrize("k", [4, 5])
+@pytest.mark.parametrize("k", [4, 5, 6])
 def test_headline_fused_fp32_matches_reference(golden, k):
     nat = native()
     h = run_headline(golden, nat.ENGINE_FUSED, precision=nat.SVB_FP32, fusion_width=k)

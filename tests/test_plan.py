@@ -143,6 +143,63 @@ def test_fused_plan_rejects_srn(emu):
     assert rc == -3
 
 
+def run_fused6_emu(lib, n, gates):
+    re = np.zeros(1 << n)
+    im = np.zeros(1 << n)
+    re[0] = 1.0
+    a = ctypes.c_uint64()
+    rc = lib.emu_fused6_run(n, gates.ctypes.data, ctypes.c_size_t(len(gates)), re.ctypes.data_as(_dp),
+                            im.ctypes.data_as(_dp), ctypes.byref(a))
+    return rc, re, im, a.value
+
+
+@pytest.mark.parametrize("n,depth", [(12, 6), (13, 5), (15, 4), (16, 3)])
+def test_fused6_plan_random_matching(emu, oracle, n, depth):
+    """Fusion width 6: greedy 6-qubit blocks (one per pass), the B-operand plane offsets,
+    the canonical K-major reads of the MMA and the output offsets, executed on the CPU
+    (MMA in FP64): only the TF32 hi + lo rounding of the gate remains."""
+    g = circuits.random_matching_circuit(n, depth, seed=n * 11 + depth)
+    rc, re, im, passes = run_fused6_emu(emu, n, g)
+    assert rc == 0
+    ore, oim = oracle.run(n, g)
+    assert 1 - fidelity(re + 1j * im, ore + 1j * oim) < 1e-12
+    assert np.max(np.abs(re - ore)) < 1e-7 and passes < len(g)
+
+
+def test_fused6_plan_every_op_but_srn(emu, oracle):
+    n = 13
+    g = mixed_circuit(n, 3, seed=33)
+    g = g[g["op"] != G.OP["SRN"]]
+    rc, re, im, _ = run_fused6_emu(emu, n, g)
+    assert rc == 0
+    ore, oim = oracle.run(n, g)
+    assert 1 - fidelity(re + 1j * im, ore + 1j * oim) < 1e-12
+
+
+def test_fused6_plan_low_qubit_targets(emu, oracle):
+    """Blocks whose targets include qubits 0 and 1 (both targets: the 2-way-conflict
+    layout), only qubit 0, or neither, and blocks padded to 6 targets."""
+    gl = []
+    for q in range(12):
+        gl.append(G.U3(0.3 + 0.1 * q, 0.2 * q, -0.4, q))
+    gl += [G.CX(0, 1), G.CX(1, 5), G.CX(0, 7), G.U3(0.5, 0.1, 0.2, 0), G.CX(2, 3), G.CX(9, 11),
+           G.CX(4, 13), G.H(12), G.CX(12, 0), G.RZ(0.7, 1), G.CX(10, 2)]
+    g = G.to_array(gl)
+    rc, re, im, _ = run_fused6_emu(emu, 14, g)
+    assert rc == 0
+    ore, oim = oracle.run(14, g)
+    assert 1 - fidelity(re + 1j * im, ore + 1j * oim) < 1e-12
+
+
+def test_fused6_plan_headline_circuit_blocks(emu):
+    """n = 30, depth 40: 1,800 gates in at most 180 six-qubit blocks (passes)."""
+    g = circuits.random_matching_circuit(30, 40, seed=2024)
+    a, b = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = emu.emu_fused_stats(30, g.ctypes.data, ctypes.c_size_t(len(g)), 6, ctypes.byref(a), ctypes.byref(b))
+    assert rc == 0
+    assert a.value == b.value and a.value <= 180
+
+
 def run_pairs_emu(lib, n, gates):
     re = np.zeros(1 << n)
     im = np.zeros(1 << n)
