@@ -382,19 +382,17 @@ k_fused(float2* __restrict__ sv, const FusedPass* __restrict__ passes,
             if (tid == 0) counts[2 + s]++;
             const float4* t4 = reinterpret_cast<const float4*>(T);
             if (blk + 1 < nb) {
-                // this thread's rows of the next block
+                // this thread's rows of the next block, one 8-byte read per amplitude at its
+                // transpose slot (the 16 lanes of a half warp, rows n..n+15, hit 16 bank
+                // pairs: fused_slot puts row bits 0..2 on the chunk and row bit 3 on the word)
 #pragma unroll
                 for (int mb = 0; mb < MBLK; mb++) {
                     const uint32_t n = (uint32_t)(128 * mb + 32 * quad + lane);
-                    const bool swap = (n >> 3) & 1u;       // fused_slot swaps a chunk's amplitudes
 #pragma unroll
-                    for (int c2 = 0; c2 < CA / 2; c2++) {
-                        const uint32_t c = (uint32_t)(part * (CA / 2) + c2);
-                        const float4 x = t4[n * CPR + (c ^ fused_chunk_swizzle(n, K))];
-                        v[mb][4 * c2] = swap ? x.z : x.x;
-                        v[mb][4 * c2 + 1] = swap ? x.w : x.y;
-                        v[mb][4 * c2 + 2] = swap ? x.x : x.z;
-                        v[mb][4 * c2 + 3] = swap ? x.y : x.w;
+                    for (int a2 = 0; a2 < CA; a2++) {
+                        const float2 x = T[fused_slot(n, (uint32_t)(part * CA + a2), K)];
+                        v[mb][2 * a2] = x.x;
+                        v[mb][2 * a2 + 1] = x.y;
                     }
                 }
                 blk++;
