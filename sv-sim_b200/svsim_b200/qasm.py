@@ -19,8 +19,12 @@ compile step:
 * parameters are arithmetic expressions over numbers, ``pi`` and sin/cos/tan/exp/ln/
   sqrt, evaluated with a restricted evaluator (no Python ``eval``);
 * ``measure`` records (qubit, classical bit) pairs; ``barrier``, ``creg``, ``include``
-  and the ``OPENQASM`` header carry no gate.  ``reset``, ``if`` and ``opaque`` have no
-  counterpart in this engine's circuits and are rejected with an error naming the line.
+  and the ``OPENQASM`` header carry no gate;
+* ``reset``, an ``if (...)`` statement with the gate it conditions, and ``opaque`` have no
+  counterpart in the reference's state-vector circuits: its translator drops those
+  statements whole (its ``other_keys`` list, :104, skipped at :325-326), and so does this
+  loader by default, recording each one in ``QasmProgram.skipped``.  With
+  ``strict=True`` they are rejected instead, with an error naming the line.
 """
 from __future__ import annotations
 
@@ -122,6 +126,7 @@ class QasmProgram:
     gates: np.ndarray                                   # GATE_DTYPE records
     qregs: dict[str, tuple[int, int]] = field(default_factory=dict)   # name -> (offset, size)
     measured: list[tuple[int, str, int]] = field(default_factory=list)  # (qubit, creg, bit)
+    skipped: list[tuple[int, str]] = field(default_factory=list)        # (line, statement)
 
 
 _CALL = re.compile(r"^([A-Za-z_][A-Za-z0-9_]*)\s*(\((.*)\))?\s*(.*)$", re.S)
@@ -157,9 +162,11 @@ def _statements(text: str) -> list[tuple[int, str]]:
     return out
 
 
-def loads(text: str) -> QasmProgram:
-    """Parses an OpenQASM 2.0 program."""
+def loads(text: str, strict: bool = False) -> QasmProgram:
+    """Parses an OpenQASM 2.0 program.  ``reset``, ``if`` and ``opaque`` statements are
+    dropped as the reference's translator drops them (``strict=False``) or rejected."""
     qregs: dict[str, tuple[int, int]] = {}
+    skipped: list[tuple[int, str]] = []
     gate_defs: dict[str, GateDef] = {}
     rows: list = []
     measured: list[tuple[int, str, int]] = []
@@ -227,8 +234,12 @@ def loads(text: str) -> QasmProgram:
             continue
         if head in ("include", "creg", "barrier"):
             continue
-        if head in ("reset", "if", "opaque"):
-            raise QasmError(f"line {line}: {head!r} is not supported")
+        word = re.match(r"[A-Za-z_][A-Za-z0-9_]*", head)
+        if word and word.group(0) in ("reset", "if", "opaque"):
+            if strict:
+                raise QasmError(f"line {line}: {word.group(0)!r} is not supported")
+            skipped.append((line, st))
+            continue
         if head == "qreg":
             m = re.fullmatch(r"qreg\s+([A-Za-z_][A-Za-z0-9_]*)\s*\[\s*(\d+)\s*\]", st)
             if not m:
@@ -278,9 +289,9 @@ def loads(text: str) -> QasmProgram:
     arr = np.zeros(len(rows), dtype=G.GATE_DTYPE)
     for i, r in enumerate(rows):
         arr[i] = r
-    return QasmProgram(n_qubits, arr, qregs, measured)
+    return QasmProgram(n_qubits, arr, qregs, measured, skipped)
 
 
-def load(path: str) -> QasmProgram:
+def load(path: str, strict: bool = False) -> QasmProgram:
     with open(path, encoding="utf-8") as f:
-        return loads(f.read())
+        return loads(f.read(), strict=strict)

@@ -100,7 +100,6 @@ def test_expressions():
 @pytest.mark.parametrize("bad,msg", [
     ("OPENQASM 2.0; qreg q[2]; foo q[0];", "unknown gate"),
     ("OPENQASM 2.0; qreg q[2]; h q[2];", "outside register"),
-    ("OPENQASM 2.0; qreg q[2]; reset q[0];", "not supported"),
     ("OPENQASM 2.0; qreg q[2]; cx q[0], q[0];", "repeats a qubit"),
     ("OPENQASM 2.0; qreg q[2]; u3(1, 2) q[0];", "parameters"),
     ("OPENQASM 2.0; qreg q[2]; qreg r[3]; cx q, r;", "different sizes"),
@@ -110,3 +109,18 @@ def test_expressions():
 def test_errors_name_the_problem(bad, msg):
     with pytest.raises(QasmError, match=msg):
         loads(bad)
+
+
+def test_reset_if_opaque_dropped_as_the_reference_translator_does():
+    """The reference's translator drops `reset`, `if (...) <gate>` and unknown statements
+    whole (svsim_qasm_cplus.py:104, :325-326); the loader does the same by default and
+    records them, and rejects them with strict=True."""
+    src = ("OPENQASM 2.0;\ninclude \"qelib1.inc\";\nqreg q[2];\ncreg c[2];\nh q[0];\nreset q[1];\n"
+           "measure q[0] -> c[0];\nif(c==1) x q[1];\nif (c == 0) cx q[0], q[1];\ncx q[0], q[1];\n")
+    prog = loads(src)
+    assert [int(g["op"]) for g in prog.gates] == [G.OP["H"], G.OP["CX"]]
+    assert [ln for ln, _ in prog.skipped] == [6, 8, 9]
+    assert prog.skipped[1][1].replace(" ", "") == "if(c==1)xq[1]"
+    for bad in ("OPENQASM 2.0; qreg q[2]; reset q[0];", "OPENQASM 2.0; qreg q[1]; creg c[1]; if(c==1) x q[0];"):
+        with pytest.raises(QasmError, match="not supported"):
+            loads(bad, strict=True)
