@@ -165,9 +165,37 @@ struct PassPairs {
     Pend pend[NSLOT];
     Scalar ph;
 
+    // after . (pend[x] (x) pend[y]) folded into the last block when that block acts on the
+    // same two positions: every op on x or y since that block is pending here (a
+    // two-qubit op on either would have made a later block), so the product is that
+    // block followed by this one.  A density-matrix gate and its noise channel on
+    // (q, q + n), or CX . U1 . CX on one pair, become one block instead of two.
+    bool merge_last(int x, int y, const M4* after)
+    {
+        if (blocks.empty()) return false;
+        Block& L = blocks.back();
+        const bool same = L.x == x && L.y == y, swapped = L.x == y && L.y == x;
+        if (!same && !swapped) return false;
+        const std::vector<int> cond = cond_union(L.cond, cond_union(pend[x].cond, pend[y].cond));
+        if (cond.size() > (size_t)PR_MAX_COND) return false;
+        std::vector<M4> nv((size_t)1 << cond.size());
+        for (size_t u = 0; u < nv.size(); u++) {
+            M4 m = kron(pend[x].v[sub_index(cond, (int)u, pend[x].cond)],
+                        pend[y].v[sub_index(cond, (int)u, pend[y].cond)]);
+            if (after) m = mul4(*after, m);
+            if (swapped) m = swap_bits(m);         // into the last block's bit order
+            nv[u] = mul4(m, L.v[sub_index(cond, (int)u, L.cond)]);
+        }
+        L.cond = cond;
+        L.v = nv;
+        pend[x] = Pend{};
+        pend[y] = Pend{};
+        return true;
+    }
     // block = after . (pend[x] (x) pend[y]), plus the pending tile phase when it fits
     void close(int x, int y, const M4* after)
     {
+        if (merge_last(x, y, after)) return;
         Block b;
         b.x = x;
         b.y = y;
