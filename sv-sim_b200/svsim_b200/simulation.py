@@ -46,17 +46,21 @@ class Simulation:
 
     @classmethod
     def from_qasm(cls, source: str, i_gpu: int = 0, precision: str = "fp64",
-                  engine: int = ENGINE_AUTO, tile_bits: int = 0) -> "Simulation":
+                  engine: int = ENGINE_AUTO, tile_bits: int = 0, strict: bool = False) -> "Simulation":
         """A Simulation holding an OpenQASM 2.0 program (a file path or the program text),
         with one qubit per declared qubit (registers in declaration order).  The
-        program's measure records are kept in ``qasm_measured``."""
+        program's measure records are kept in ``qasm_measured`` and the statements dropped
+        as the reference's translator drops them (reset, if, opaque) in ``qasm_skipped``;
+        ``strict=True`` rejects those instead."""
         import os
         from . import qasm
-        prog = qasm.load(source) if os.path.isfile(source) else qasm.loads(source)
+        prog = (qasm.load(source, strict=strict) if os.path.isfile(source)
+                else qasm.loads(source, strict=strict))
         sim = cls(prog.n_qubits, i_gpu, precision, engine, tile_bits)
         for g in _g.from_array(prog.gates):
             sim.append(g)
         sim.qasm_measured = prog.measured
+        sim.qasm_skipped = prog.skipped
         return sim
 
     # ---- circuit ----------------------------------------------------------------------
