@@ -194,6 +194,15 @@ svb_status svb_measure(svb_sim* sim, const double* uniforms, uint32_t shots,
 svb_status svb_measure_seeded(svb_sim* sim, uint32_t seed, uint32_t shots, uint64_t* out,
                               double* prob_total);
 
+/* Self-test of the bounded waits the persistent kernels rely on (no reference counterpart:
+ * the reference's grid.sync() in simulation_kernel, svsim_nvgpu_sin.cuh:614-621, waits
+ * without limit).  One kernel waits on an mbarrier nothing arrives at, with the fused
+ * engines' tensor-core completion wait (it gives up after 2 s); one waits at a grid
+ * barrier whose arrival count is never reached, with the batched engines' barrier (it
+ * gives up after more than 1 s).  Each must give up and report it, and the context must
+ * stay usable: *mbar_timed_out and *grid_timed_out receive 1 when the wait gave up. */
+svb_status svb_selftest_waits(int device, int* mbar_timed_out, int* grid_timed_out);
+
 /* Largest state size svb_measure_noalloc accepts. */
 #define SVB_NOALLOC_MAX_QUBITS 30
 

@@ -511,6 +511,19 @@ __global__ void k_cost_table(const QaoaDesc* inst, int n_inst, const uint32_t* e
 }
 
 }  // namespace
+// One CTA arrives at a grid barrier whose target (two arrivals) is never reached: the
+// bounded wait of grid_barrier gives up and raises bar[1] (the batched kernels' error flag).
+__global__ void k_grid_barrier_probe(unsigned* bar)
+{
+    grid_barrier(bar, 2u);
+}
+
+cudaError_t launch_grid_barrier_probe(unsigned* bar, cudaStream_t s)
+{
+    k_grid_barrier_probe<<<1, 32, 0, s>>>(bar);
+    return cudaGetLastError();
+}
+
 }  // namespace svb
 
 // ---------------------------------------------------------------------------------------

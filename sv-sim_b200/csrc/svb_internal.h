@@ -350,6 +350,12 @@ struct DevFusedBuffers {
 cudaError_t launch_fused_pass(void* state, int n, int k, int pass_index, int n_blocks,
                               int gate_words_per_block, const DevFusedBuffers& b, cudaStream_t s);
 cudaError_t launch_fused6_pass(void* state, int n, int pass_index, const DevFusedBuffers& b, cudaStream_t s);
+
+// Self-test of the bounded device waits (selftest.cu, batch.cu): the grid barrier of the
+// batched kernels on a target never reached (sets bar[1]); the mbarrier wait of the fused
+// kernels on a barrier nothing arrives at (writes 1 to *flag when it gives up).
+cudaError_t launch_grid_barrier_probe(unsigned* bar, cudaStream_t s);
+cudaError_t launch_mbarrier_probe(int* flag, cudaStream_t s);
 // Rescales the FP32 state to unit norm (norm summed in FP64) after a fused run.
 cudaError_t launch_fused_renorm(void* state, int n, const DevFusedBuffers& b, cudaStream_t s);
 

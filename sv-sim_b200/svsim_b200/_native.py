@@ -109,6 +109,8 @@ _SIGS = {
     "svb_version": ([], ctypes.c_char_p),
     "svb_fp64_mma_peak": ([ctypes.c_int, _dp], ctypes.c_int),
     "svb_l2_copy_peak": ([ctypes.c_int, _dp], ctypes.c_int),
+    "svb_selftest_waits": ([ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+                           ctypes.c_int),
 }
 
 
@@ -142,6 +144,14 @@ def fp64_mma_peak(device: int = 0) -> float:
     v = ctypes.c_double()
     check(lib().svb_fp64_mma_peak(device, ctypes.byref(v)))
     return v.value
+
+
+def selftest_waits(device: int = 0) -> tuple[bool, bool]:
+    """(mbarrier wait gave up, grid barrier gave up) for waits made to run out on purpose
+    (svb_selftest_waits); both must be True."""
+    m, g = ctypes.c_int(), ctypes.c_int()
+    check(lib().svb_selftest_waits(device, ctypes.byref(m), ctypes.byref(g)))
+    return bool(m.value), bool(g.value)
 
 
 def l2_copy_peak(device: int = 0) -> float:
