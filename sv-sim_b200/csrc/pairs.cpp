@@ -164,6 +164,7 @@ struct PassPairs {
     std::vector<Block> blocks;
     Pend pend[NSLOT];
     Scalar ph;
+    bool no_merge = false;           // set while a close must emit the pending tile phase
 
     // after . (pend[x] (x) pend[y]) folded into the last block when that block acts on the
     // same two positions: every op on x or y since that block is pending here (a
@@ -172,7 +173,7 @@ struct PassPairs {
     // (q, q + n), or CX . U1 . CX on one pair, become one block instead of two.
     bool merge_last(int x, int y, const M4* after)
     {
-        if (blocks.empty()) return false;
+        if (blocks.empty() || no_merge) return false;
         Block& L = blocks.back();
         const bool same = L.x == x && L.y == y, swapped = L.x == y && L.y == x;
         if (!same && !swapped) return false;
@@ -246,7 +247,9 @@ struct PassPairs {
             Pend a = pend[0], b = pend[1];
             pend[0] = Pend{};
             pend[1] = Pend{};
+            no_merge = true;           // a block of its own, which takes the phase
             close(0, 1, nullptr);
+            no_merge = false;
             pend[0] = a;
             pend[1] = b;
         }
@@ -300,7 +303,11 @@ struct PassPairs {
                 flush(open[i]);
             }
         }
-        if (ph.active) flush(0);       // pend[0] is idle here: a block with only the phase
+        if (ph.active) {               // pend[0] is idle here: a block with only the phase
+            no_merge = true;
+            flush(0);
+            no_merge = false;
+        }
     }
 };
 

@@ -356,8 +356,8 @@ extern "C" int emu_fused_stats(uint32_t n, const svb_gate* gates, size_t n_gates
 // PO_SWAP as the warp-shuffle exchange, PO_RELAYOUT through the swizzled shared tile
 // (every slot written once), PO_BLOCK as the mma.sync m8n8k4 fragment rules (thread t
 // holds A[t>>2][t&3] and B[t&3][t>>2], receives D[t>>2][2(t&3)], D[t>>2][2(t&3)+1]).
-extern "C" int emu_pairs_run(uint32_t n, const svb_gate* gates, size_t n_gates, double* re, double* im,
-                             uint64_t* stats)
+static int pairs_run(uint32_t n, const svb_gate* gates, size_t n_gates, double* re, double* im,
+                     uint64_t* stats, bool from_input)
 {
     std::vector<EOp> eops;
     for (size_t i = 0; i < n_gates; i++)
@@ -368,6 +368,8 @@ extern "C" int emu_pairs_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
     std::vector<double2> sv(1ull << n);
     for (auto& a : sv) a = make_double2(0, 0);
     sv[0] = make_double2(1, 0);
+    if (from_input)
+        for (uint64_t i = 0; i < sv.size(); i++) sv[i] = make_double2(re[i], im[i]);
     std::vector<double2> regs((size_t)NT * NR), sm(4096);
     std::vector<int> written(4096);
     const uint64_t tiles = 1ull << (n - PR_TILE_BITS);
@@ -514,6 +516,21 @@ extern "C" int emu_pairs_run(uint32_t n, const svb_gate* gates, size_t n_gates, 
 }
 
 // Plan statistics of the pair engine (no execution): passes, blocks, swaps, relayouts.
+
+// A pair plan run thread by thread from |0..0> (re, im out).
+extern "C" int emu_pairs_run(uint32_t n, const svb_gate* gates, size_t n_gates, double* re, double* im,
+                             uint64_t* stats)
+{
+    return pairs_run(n, gates, n_gates, re, im, stats, false);
+}
+
+// The same from the state in re, im (in and out): a plan must be right on any input state.
+extern "C" int emu_pairs_run_from(uint32_t n, const svb_gate* gates, size_t n_gates, double* re, double* im,
+                                  uint64_t* stats)
+{
+    return pairs_run(n, gates, n_gates, re, im, stats, true);
+}
+
 extern "C" int emu_pairs_stats(uint32_t n, const svb_gate* gates, size_t n_gates, uint64_t* stats)
 {
     std::vector<EOp> eops;

@@ -273,3 +273,97 @@ def test_pair_plan_cx_dense_vs_oracle(emu, oracle):
     assert rc == 0, rc
     ore, oim = oracle.run(12, g)
     assert np.max(np.abs((re + 1j * im) - (ore + 1j * oim))) < 1e-13
+
+
+# ---- every plan on a random input state -------------------------------------------------
+# From |0..0>, an op that only multiplies amplitudes with some qubit at 1 (a phase on a
+# non-local qubit, a tile-selected variant) is invisible until the state spreads; a plan that
+# drops one passes every test that starts there.  These run each planner on circuits heavy
+# in diagonal ops, from a random normalised state, against the oracle applied to that state.
+
+def random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    s = rng.normal(size=(2, 1 << n))
+    s /= np.sqrt((s ** 2).sum())
+    return s[0].copy(), s[1].copy()
+
+
+def diagonal_heavy_circuit(n, m, seed):
+    rng = np.random.default_rng(seed)
+    gl = []
+    for _ in range(m):
+        r = rng.random()
+        q = int(rng.integers(n))
+        q2 = int(rng.integers(n - 1))
+        q2 += q2 >= q
+        if r < 0.3:
+            gl.append(G.RZ(rng.uniform(-3, 3), q))
+        elif r < 0.4:
+            gl.append(G.T(q))
+        elif r < 0.5:
+            gl.append(G.U1(rng.uniform(-3, 3), q))
+        elif r < 0.65:
+            gl.append(G.CX(q, q2))
+        elif r < 0.75:
+            gl.append(G.CZ(q, q2))
+        elif r < 0.85:
+            gl.append(G.RY(rng.uniform(-3, 3), q))
+        else:
+            gl.append(G.U3(*rng.uniform(-3, 3, 3), q))
+    return G.to_array(gl)
+
+
+def ansatz_segment(n, lo, hi):
+    """Ops lo..hi of the hardware-efficient ansatz: a segment that opens with a run of RZ
+    (the adjoint's forward checkpoints cut the circuit like this)."""
+    pc = circuits.hardware_efficient_ansatz(n=n, layers=2, seed=7)
+    return np.ascontiguousarray(pc.evaluated(pc.params)[lo:hi])
+
+
+STATE_CASES = [(n, diagonal_heavy_circuit(n, m, seed)) for n, m, seed in
+               ((12, 60, 1), (13, 40, 2), (14, 80, 3), (15, 50, 4), (17, 90, 5))]
+# n = 18, a pass of 12 local qubits: the segment's first RZ on 5 or more non-local qubits
+# fill the tile phase twice over before any block
+STATE_CASES += [(18, ansatz_segment(18, 22, 46)), (18, ansatz_segment(18, 58, 82))]
+
+
+@pytest.mark.parametrize("case", range(len(STATE_CASES)))
+def test_pair_plan_on_random_state(emu, oracle, case):
+    n, g = STATE_CASES[case]
+    re, im = random_state(n, case)
+    ore, oim = oracle.run(n, g, state=(re, im))
+    st = np.zeros(4, dtype=np.uint64)
+    vp = ctypes.c_void_p
+    rc = emu.emu_pairs_run_from(ctypes.c_uint32(n), vp(g.ctypes.data), ctypes.c_size_t(len(g)),
+                                vp(re.ctypes.data), vp(im.ctypes.data), vp(st.ctypes.data))
+    assert rc == 0
+    assert np.max(np.abs((re + 1j * im) - (ore + 1j * oim))) < 1e-13
+
+
+@pytest.mark.parametrize("case", range(len(STATE_CASES)))
+def test_staged_plan_on_random_state(emu, oracle, case):
+    n, g = STATE_CASES[case]
+    st = random_state(n, case)
+    ore, oim = oracle.run(n, g, state=st)
+    for M in (10, 12):
+        re, im, _ = run_emu(emu, n, g, M, state=st)
+        assert np.max(np.abs((re + 1j * im) - (ore + 1j * oim))) < 1e-13, M
+
+
+@pytest.mark.parametrize("case", range(len(STATE_CASES)))
+def test_fused_plans_on_random_state(emu, oracle, case):
+    n, g = STATE_CASES[case]
+    st = random_state(n, case)
+    ore, oim = oracle.run(n, g, state=st)
+    for k in (3, 4, 5, 6):
+        re, im = st[0].copy(), st[1].copy()
+        if k < 6:
+            a, b = ctypes.c_uint64(), ctypes.c_uint64()
+            rc = emu.emu_fused_run(n, g.ctypes.data, ctypes.c_size_t(len(g)), k, re.ctypes.data_as(_dp),
+                                   im.ctypes.data_as(_dp), ctypes.byref(a), ctypes.byref(b))
+        else:
+            a = ctypes.c_uint64()
+            rc = emu.emu_fused6_run(n, g.ctypes.data, ctypes.c_size_t(len(g)), re.ctypes.data_as(_dp),
+                                    im.ctypes.data_as(_dp), ctypes.byref(a))
+        assert rc == 0, k
+        assert 1 - fidelity(re + 1j * im, ore + 1j * oim) < 1e-12, k
