@@ -762,8 +762,9 @@ def tuning_form(device):
 def batch_form(device, reps=5):
     """Batched circuits in one graph-replayed persistent launch (svb_cbatch_*): 64
     parameter points of the n=20, 480-parameter ansatz with their energies, and 128
-    random circuits with n ~ U{10..22}; the autotuned tile/block choice next to the fixed
-    default (12-qubit tiles, 512 threads)."""
+    random circuits with n ~ U{10..22}; the autotuned choice next to the fixed shared-memory
+    sweep (12-qubit tiles, 512 threads) and the pair engine (FP64 tensor-core blocks for the
+    circuits of 12 or more qubits, the sweep for the rest)."""
     import torch
     from svsim_b200 import circuits, _native as nat
     pc = circuits.hardware_efficient_ansatz()
@@ -778,7 +779,7 @@ def batch_form(device, reps=5):
     for name, batch, tb in (("ansatz_points_64", [(20, pc.evaluated(p)) for p in pts], None),
                             ("random_mixed_128", mixed, None)):
         res = {}
-        for label, tile in (("tuned", 0), ("fixed_tile12", 12)):
+        for label, tile in (("tuned", 0), ("fixed_tile12", 12), ("pairs", nat.CBATCH_PAIRS)):
             t0 = time.perf_counter()
             b = nat.CircuitBatch(batch, [terms] * len(batch) if name.startswith("ansatz") else None,
                                  device=device, tile_bits=tile)
@@ -794,7 +795,8 @@ def batch_form(device, reps=5):
             res[label] = {"circuits_per_s": len(batch) / sec, "ms_per_batch": sec * 1e3,
                           "gates_per_s": gates / sec, "tile_bits": int(st.tile_bits), "threads": int(st.threads),
                           "phases": int(st.n_phases), "graphed": bool(st.graphed), "grid": int(st.grid),
-                          "state_gbs": st.moved_bytes / sec / 1e9, "setup_s": setup}
+                          "state_gbs": st.moved_bytes / sec / 1e9, "setup_s": setup,
+                          "pair_circuits": int(st.pair_circuits)}
             b.close()
             torch.cuda.empty_cache()
         out[name] = res

@@ -364,10 +364,16 @@ svb_status svb_qaoa_destroy(svb_qaoa_batch* batch);
  * (svsim_nvgpu_sin.cuh:193-339) with its fixed launch shape (:309-316, config.hpp:48).
  * Circuit i's gates are gates[gate_offsets[i] .. gate_offsets[i+1]); its observable (may be
  * empty) terms[term_offsets[i] .. term_offsets[i+1]) (term_offsets may be NULL: no
- * energies).  tile_bits (local qubits of a work tile, 6..12 FP64, 6..13 FP32) 0 = chosen by
- * the autotuner: the candidate tile sizes and block sizes are timed on the batch itself and
- * the fastest kept; the choice is cached per batch shape (precision, device, qubit and gate
- * counts) for later batches of that shape. */
+ * energies).  tile_bits: the local qubits of a shared-memory sweep tile (6..12 FP64, 6..13
+ * FP32), every op one sweep of the tile; SVB_CBATCH_PAIRS = the pair engine (FP64
+ * two-qubit blocks on the tensor cores, 4,096-amplitude tiles) for every FP64 circuit of
+ * 12 or more qubits it can run (no SRN), 12-qubit sweep tiles for the others; 0 = chosen by
+ * the autotuner: these candidates (three tile sizes and two block sizes of the sweep, and
+ * the pair engine) are timed on the batch itself and the fastest kept; the choice is cached
+ * per batch shape (precision, device, qubit and gate counts) for later batches of that
+ * shape. */
+#define SVB_CBATCH_PAIRS (-1)
+
 typedef struct svb_circuit_batch svb_circuit_batch;
 
 typedef struct {
@@ -381,7 +387,11 @@ typedef struct {
     uint32_t graphed;             /* 1 if a run replays a CUDA graph */
     double moved_bytes;           /* state bytes one run reads and writes (passes x 2 x state) */
     uint32_t tuned;               /* 1 if the autotuner chose tile_bits and threads */
-    uint32_t n_passes;
+    uint32_t n_passes;            /* sweep passes of all circuits */
+    uint32_t pair_circuits;       /* circuits run by the pair engine */
+    uint32_t pair_passes;         /* their passes */
+    uint32_t pair_phases;         /* phases of the pair launch */
+    uint32_t pair_grid;           /* resident CTAs of the pair launch */
 } svb_cbatch_stats;
 
 svb_status svb_cbatch_create(int device, int precision, uint32_t n_circuits, const uint32_t* n_qubits,

@@ -20,6 +20,14 @@
 // After the last phase, each circuit's energy sum_t c_t Re <psi| P_t |psi> is summed per
 // chunk of 4,096 amplitudes by one warp each and per circuit in a fixed order (FP64,
 // repeatable).
+//
+// FP64 circuits of 12 or more qubits can instead run on the pair engine's machinery
+// (pairs_core.cuh): each is planned by plan_pairs (two-qubit blocks on the FP64 tensor
+// cores, 4,096-amplitude tiles), the plans are concatenated, and a second persistent
+// cooperative launch k_cb_pairs runs phase p = pass p of every such circuit, a CTA taking a
+// contiguous run of (circuit, pass, tile) items so that it stages a pass's ops, layouts and
+// gate fragments in shared memory once for many tiles.  That launch goes first; the sweep
+// launch then runs the other circuits and the energies of all.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -27,9 +35,11 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <tuple>
 #include <vector>
 
-#include "gate_math.cuh"
+#include "pairs_core.cuh"
 
 namespace svb {
 namespace {
@@ -284,7 +294,73 @@ __global__ void k_cb_ones(void* pool, const CbCircuit* circ, int n_circ)
     }
 }
 
+struct CbPairArgs {
+    double2* pool;
+    const CbCircuit* circ;
+    const PairPass* passes;
+    const PairOp* ops;
+    const DevStage* layouts;
+    const double2* gates;
+    const CbItem* items;
+    const uint32_t* phase_off;   // [n_phases + 1]
+    unsigned* barrier;           // [0] arrivals (zeroed before each launch), [1] error flag
+    int n_phases;
+    int pad;
+};
+
+// Phase p runs pass p of every pair-planned circuit.  The items of a phase are ordered by
+// circuit and tile, and each CTA takes a contiguous share of them, so it changes pass (and
+// stages the new pass's data) at most a few times per phase.
+__global__ void __launch_bounds__(PR_THREADS, 2) k_cb_pairs(CbPairArgs A)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    __shared__ PairPass sP;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    int cur = -1;
+    PairStaged S{};
+    PairGOffs gin{}, gout{};
+    unsigned target = 0;
+    for (int ph = 0; ph < A.n_phases; ph++) {
+        const uint32_t lo = A.phase_off[ph];
+        const uint64_t cnt = A.phase_off[ph + 1] - lo;
+        const uint32_t b0 = lo + (uint32_t)(cnt * blockIdx.x / gridDim.x);
+        const uint32_t b1 = lo + (uint32_t)(cnt * (blockIdx.x + 1) / gridDim.x);
+        for (uint32_t it = b0; it < b1; it++) {
+            const CbItem item = A.items[it];
+            if ((int)item.pass != cur) {
+                __syncthreads();       // every thread is done with the previous pass's data
+                const uint32_t* src = reinterpret_cast<const uint32_t*>(A.passes + item.pass);
+                uint32_t* dst = reinterpret_cast<uint32_t*>(&sP);
+                for (int w = tid; w < (int)(sizeof(PairPass) / 4); w += PR_THREADS) dst[w] = src[w];
+                __syncthreads();
+                S = pair_stage(smem_raw, sP, A.ops, A.layouts, A.gates, tid);
+                pair_goffs(S.lay[0], sP.local_q, tid, gin);
+                pair_goffs(S.lay[S.n_lay - 1], sP.local_q, tid, gout);
+                cur = (int)item.pass;
+            }
+            pair_tile(A.pool + A.circ[item.circuit].state_off, sm, sP, S, gin, gout, item.tile, tid, lane);
+        }
+        target += gridDim.x;
+        cb_grid_barrier(A.barrier, target);
+    }
+}
+
 // ---- host side ----------------------------------------------------------------------
+
+// The pair-engine part of a batch plan: the circuits' pair plans concatenated (indices
+// rebased), and the (circuit, pass, tile) items of each phase.
+struct CbPairPlan {
+    std::vector<PairPass> passes;
+    std::vector<PairOp> ops;
+    std::vector<DevStage> layouts;
+    std::vector<double> gates;
+    std::vector<CbItem> items;
+    std::vector<uint32_t> phase_off;
+    size_t stage_bytes = 0;
+    uint32_t circuits = 0;
+};
 
 struct CbPlan {
     std::vector<CbCircuit> circ;
@@ -295,6 +371,7 @@ struct CbPlan {
     std::vector<uint32_t> chunk_circ;
     uint64_t pool_amps = 0;
     double moved_bytes = 0;
+    CbPairPlan pairs;
 };
 
 CbPass make_pass(uint64_t L, int n)
@@ -359,6 +436,7 @@ struct svb_circuit_batch {
     uint32_t n_circ = 0;
     int tile_bits = 12;
     int threads = 512;
+    bool use_pairs = false;      // pair engine for the FP64 circuits of >= 12 qubits
     bool tuned = false;
     std::vector<uint32_t> n;
     std::vector<uint64_t> gate_off;
@@ -377,16 +455,25 @@ struct svb_circuit_batch {
     uint32_t* d_chunk_circ = nullptr;
     double* d_partial = nullptr;
     double* d_energy = nullptr;
-    unsigned* d_bar = nullptr;
+    unsigned* d_bar = nullptr;   // [0, 1] the sweep launch's barrier, [2, 3] the pair launch's
+    svb::PairPass* d_ppasses = nullptr;
+    svb::PairOp* d_pops = nullptr;
+    svb::DevStage* d_playouts = nullptr;
+    double* d_pgates = nullptr;
+    svb::CbItem* d_pitems = nullptr;
+    uint32_t* d_pphase_off = nullptr;
     // pinned host
     svb::CbOp* h_ops = nullptr;
+    double* h_pgates = nullptr;
     double* h_energy = nullptr;
-    unsigned* h_err = nullptr;
+    unsigned* h_err = nullptr;   // the 4 barrier words after a run
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool graphed = false;
     unsigned grid = 0;
     size_t smem = 0;
+    unsigned pgrid = 0;
+    size_t psmem = 0;
 };
 
 namespace svb {
@@ -408,19 +495,110 @@ void cb_free(svb_circuit_batch* b)
     cudaFree(b->d_partial);
     cudaFree(b->d_energy);
     cudaFree(b->d_bar);
+    cudaFree(b->d_ppasses);
+    cudaFree(b->d_pops);
+    cudaFree(b->d_playouts);
+    cudaFree(b->d_pgates);
+    cudaFree(b->d_pitems);
+    cudaFree(b->d_pphase_off);
     cudaFreeHost(b->h_ops);
+    cudaFreeHost(b->h_pgates);
     cudaFreeHost(b->h_energy);
     cudaFreeHost(b->h_err);
     delete b;
 }
 
-// The plan for tile size MB; false (with a message) on an invalid gate.
-bool cb_build_plan(const svb_circuit_batch* b, const svb_gate* gates, int MB, CbPlan& plan, std::string& err)
+// Runs f(i) for i in [0, count) on up to 16 host threads.
+template <typename F>
+void cb_parallel_for(size_t count, F&& f)
+{
+    const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>({hw, (size_t)16, count});
+    if (nt <= 1) {
+        for (size_t i = 0; i < count; i++) f(i);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; t++)
+        pool.emplace_back([&, t] {
+            for (size_t i = t; i < count; i += nt) f(i);
+        });
+    for (auto& th : pool) th.join();
+}
+
+// Appends circuit c's pair plan to the batch's (indices rebased) and its items per phase;
+// false (nothing appended) when the concatenated layouts would outgrow the 16-bit indices.
+bool cb_append_pairs(CbPairPlan& P, const PairPlan& pp, uint32_t c, int n,
+                     std::vector<std::vector<CbItem>>& phase_items)
+{
+    const size_t op0 = P.ops.size(), lay0 = P.layouts.size(), g0 = P.gates.size() / 64, pass0 = P.passes.size();
+    if (lay0 + pp.layouts.size() > 65535) return false;
+    for (PairPass Q : pp.passes) {
+        Q.op_begin += (int32_t)op0;
+        Q.op_end += (int32_t)op0;
+        Q.load_layout += (int32_t)lay0;
+        Q.store_layout += (int32_t)lay0;
+        Q.gate_begin += (int32_t)g0;
+        P.passes.push_back(Q);
+    }
+    for (PairOp o : pp.ops) {
+        if (o.kind == PO_BLOCK) o.gate += (uint32_t)g0;
+        if (o.kind == PO_RELAYOUT) {
+            o.src = (uint16_t)(o.src + lay0);
+            o.layout = (uint16_t)(o.layout + lay0);
+        }
+        P.ops.push_back(o);
+    }
+    P.layouts.insert(P.layouts.end(), pp.layouts.begin(), pp.layouts.end());
+    P.gates.insert(P.gates.end(), pp.gates.begin(), pp.gates.end());
+    P.stage_bytes = std::max(P.stage_bytes, pp.stage_bytes);
+    P.circuits++;
+    const uint64_t tiles = 1ull << (n - PR_TILE_BITS);
+    for (size_t k = 0; k < pp.passes.size(); k++) {
+        if (phase_items.size() <= k) phase_items.resize(k + 1);
+        for (uint64_t t = 0; t < tiles; t++) phase_items[k].push_back(CbItem{c, (uint32_t)(pass0 + k), t});
+    }
+    return true;
+}
+
+// The plan for tile size MB (and, with use_pairs, the pair engine for every FP64 circuit
+// of at least 12 qubits that it can run); false (with a message) on an invalid gate.
+bool cb_build_plan(const svb_circuit_batch* b, const svb_gate* gates, int MB, bool use_pairs, CbPlan& plan,
+                   std::string& err)
 {
     plan = CbPlan{};
     const size_t amp = b->precision == SVB_FP64 ? 16 : 8;
-    std::vector<std::vector<uint32_t>> per_phase;     // item indices per phase, built below
-    std::vector<std::vector<CbItem>> phase_items;
+    std::vector<std::vector<EOp>> eops(b->n_circ);
+    for (uint32_t c = 0; c < b->n_circ; c++) {
+        const int n = (int)b->n[c];
+        for (uint64_t g = b->gate_off[c]; g < b->gate_off[c + 1]; g++) {
+            const svb_gate& gg = gates[g];
+            const int slots = gate_qubit_slots(gg.op);
+            if (slots == 0) { err = "gate " + std::to_string(g) + ": unknown op"; return false; }
+            for (int k = 0; k < slots; k++) {
+                if (gg.qb[k] >= (uint32_t)n) {
+                    err = "circuit " + std::to_string(c) + ", gate " + std::to_string(g) + ": qubit >= n";
+                    return false;
+                }
+                for (int j = 0; j < k; j++)
+                    if (gg.qb[j] == gg.qb[k]) { err = "gate " + std::to_string(g) + " repeats a qubit"; return false; }
+            }
+            lower_gate(gg, (int32_t)g, eops[c]);
+        }
+    }
+    // pair plans of the eligible circuits (independent: planned on several host threads)
+    std::vector<PairPlan> pp(b->n_circ);
+    std::vector<char> is_pair(b->n_circ, 0);
+    if (use_pairs && b->precision == SVB_FP64) {
+        std::vector<uint32_t> cand;
+        for (uint32_t c = 0; c < b->n_circ; c++)
+            if ((int)b->n[c] >= PR_TILE_BITS) cand.push_back(c);
+        cb_parallel_for(cand.size(), [&](size_t i) {
+            const uint32_t c = cand[i];
+            is_pair[c] = plan_pairs(eops[c], (int)b->n[c], pp[c]) ? 1 : 0;
+        });
+    }
+    std::vector<std::vector<CbItem>> phase_items, pair_items;
     uint32_t chunks = 0;
     for (uint32_t c = 0; c < b->n_circ; c++) {
         const int n = (int)b->n[c];
@@ -437,32 +615,21 @@ bool cb_build_plan(const svb_circuit_batch* b, const svb_gate* gates, int MB, Cb
         }
         plan.pool_amps += 1ull << n;
         plan.circ.push_back(C);
-        std::vector<EOp> eops;
-        for (uint64_t g = b->gate_off[c]; g < b->gate_off[c + 1]; g++) {
-            const svb_gate& gg = gates[g];
-            const int slots = gate_qubit_slots(gg.op);
-            if (slots == 0) { err = "gate " + std::to_string(g) + ": unknown op"; return false; }
-            for (int k = 0; k < slots; k++) {
-                if (gg.qb[k] >= (uint32_t)n) {
-                    err = "circuit " + std::to_string(c) + ", gate " + std::to_string(g) + ": qubit >= n";
-                    return false;
-                }
-                for (int j = 0; j < k; j++)
-                    if (gg.qb[j] == gg.qb[k]) { err = "gate " + std::to_string(g) + " repeats a qubit"; return false; }
-            }
-            lower_gate(gg, (int32_t)g, eops);
+        if (is_pair[c] && cb_append_pairs(plan.pairs, pp[c], c, n, pair_items)) {
+            plan.moved_bytes += 2.0 * amp * (double)(1ull << n) * (double)pp[c].passes.size();
+            continue;
         }
         const int M = std::min(n, MB);
         std::vector<uint32_t> my_passes;
         if (n <= MB) {
-            std::vector<int> all(eops.size());
-            for (size_t i = 0; i < eops.size(); i++) all[i] = (int)i;
+            std::vector<int> all(eops[c].size());
+            for (size_t i = 0; i < eops[c].size(); i++) all[i] = (int)i;
             my_passes.push_back((uint32_t)plan.passes.size());
-            emit_pass(plan, eops, all, n >= 64 ? ~0ull : ((1ull << n) - 1), n);
+            emit_pass(plan, eops[c], all, n >= 64 ? ~0ull : ((1ull << n) - 1), n);
         } else {
-            select_passes(eops, n, M, std::min(3, M), [&](uint64_t L, const std::vector<int>& taken) {
+            select_passes(eops[c], n, M, std::min(3, M), [&](uint64_t L, const std::vector<int>& taken) {
                 my_passes.push_back((uint32_t)plan.passes.size());
-                emit_pass(plan, eops, taken, L, n);
+                emit_pass(plan, eops[c], taken, L, n);
                 return std::vector<int>{};
             });
         }
@@ -477,6 +644,11 @@ bool cb_build_plan(const svb_circuit_batch* b, const svb_gate* gates, int MB, Cb
     for (auto& v : phase_items) {
         plan.items.insert(plan.items.end(), v.begin(), v.end());
         plan.phase_off.push_back((uint32_t)plan.items.size());
+    }
+    plan.pairs.phase_off.push_back(0);
+    for (auto& v : pair_items) {
+        plan.pairs.items.insert(plan.pairs.items.end(), v.begin(), v.end());
+        plan.pairs.phase_off.push_back((uint32_t)plan.pairs.items.size());
     }
     return true;
 }
@@ -504,12 +676,36 @@ cudaError_t cb_launch(svb_circuit_batch* b, cudaStream_t s)
     return cudaLaunchCooperativeKernel((const void*)k_cbatch<T>, dim3(b->grid), dim3(b->threads), args, b->smem, s);
 }
 
-// one evaluation: angles in, reset, launch, energies and the error flag out
+cudaError_t cb_launch_pairs(svb_circuit_batch* b, cudaStream_t s)
+{
+    CbPairArgs a;
+    a.pool = static_cast<double2*>(b->pool);
+    a.circ = b->d_circ;
+    a.passes = b->d_ppasses;
+    a.ops = b->d_pops;
+    a.layouts = b->d_playouts;
+    a.gates = reinterpret_cast<const double2*>(b->d_pgates);
+    a.items = b->d_pitems;
+    a.phase_off = b->d_pphase_off;
+    a.barrier = b->d_bar + 2;
+    a.n_phases = (int)b->plan.pairs.phase_off.size() - 1;
+    a.pad = 0;
+    void* args[] = {&a};
+    return cudaLaunchCooperativeKernel((const void*)k_cb_pairs, dim3(b->pgrid), dim3(PR_THREADS), args, b->psmem, s);
+}
+
+// one evaluation: angles in, reset, launches, energies and the error flags out
 cudaError_t cb_enqueue(svb_circuit_batch* b, cudaStream_t s)
 {
     const size_t amp = b->precision == SVB_FP64 ? 16 : 8;
-    cudaError_t e = cudaMemcpyAsync(b->d_ops, b->h_ops, b->plan.ops.size() * sizeof(CbOp), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), s);
+    const bool pairs = b->plan.pairs.circuits > 0;
+    cudaError_t e = cudaSuccess;
+    if (!b->plan.ops.empty())
+        e = cudaMemcpyAsync(b->d_ops, b->h_ops, b->plan.ops.size() * sizeof(CbOp), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && pairs && !b->plan.pairs.gates.empty())
+        e = cudaMemcpyAsync(b->d_pgates, b->h_pgates, b->plan.pairs.gates.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_bar, 0, 4 * sizeof(unsigned), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->pool, 0, b->plan.pool_amps * amp, s);
     if (e == cudaSuccess) {
         const unsigned g = (unsigned)std::min<uint64_t>((b->n_circ + 255) / 256, 1024);
@@ -517,10 +713,11 @@ cudaError_t cb_enqueue(svb_circuit_batch* b, cudaStream_t s)
         else k_cb_ones<float><<<g, 256, 0, s>>>(b->pool, b->d_circ, (int)b->n_circ);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess && pairs) e = cb_launch_pairs(b, s);
     if (e == cudaSuccess) e = b->precision == SVB_FP64 ? cb_launch<double>(b, s) : cb_launch<float>(b, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->h_energy, b->d_energy, b->n_circ * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_err, b->d_bar + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_err, b->d_bar, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, s);
     return e;
 }
 
@@ -532,12 +729,14 @@ cudaError_t upload(Tp** dst, const std::vector<Tp>& v)
     return e;
 }
 
-// Builds a batch with tile size MB and block size `threads` (device buffers, graph).
-svb_status cb_create_with(svb_circuit_batch* proto, int MB, int threads, svb_circuit_batch** out)
+// Builds a batch with tile size MB, block size `threads` and (use_pairs) the pair engine for
+// the circuits it can run: device buffers, graph.
+svb_status cb_create_with(svb_circuit_batch* proto, int MB, int threads, bool use_pairs, svb_circuit_batch** out)
 {
     svb_circuit_batch* b = new svb_circuit_batch(*proto);
     b->tile_bits = MB;
     b->threads = threads;
+    b->use_pairs = use_pairs;
     auto fail = [&](const std::string& what, cudaError_t e) {
         set_error("svb_cbatch_create: " + what + (e != cudaSuccess ? std::string(": ") + cudaGetErrorString(e) : ""));
         (void)cudaGetLastError();
@@ -545,7 +744,7 @@ svb_status cb_create_with(svb_circuit_batch* proto, int MB, int threads, svb_cir
         return e == cudaErrorMemoryAllocation ? SVB_ERR_OOM : (e == cudaSuccess ? SVB_ERR_INVALID : SVB_ERR_CUDA);
     };
     std::string err;
-    if (!cb_build_plan(b, b->gates.data(), MB, b->plan, err)) return fail(err, cudaSuccess);
+    if (!cb_build_plan(b, b->gates.data(), MB, use_pairs, b->plan, err)) return fail(err, cudaSuccess);
     const size_t amp = b->precision == SVB_FP64 ? 16 : 8;
     cudaError_t e = cudaMalloc(&b->pool, std::max<uint64_t>(1, b->plan.pool_amps) * amp);
     if (e == cudaSuccess) e = upload(&b->d_circ, b->plan.circ);
@@ -557,12 +756,21 @@ svb_status cb_create_with(svb_circuit_batch* proto, int MB, int threads, svb_cir
     if (e == cudaSuccess) e = upload(&b->d_chunk_circ, b->plan.chunk_circ);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_partial, std::max<size_t>(1, b->plan.chunk_circ.size()) * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_energy, std::max<size_t>(1, b->n_circ) * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_bar, 2 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_bar, 4 * sizeof(unsigned));
+    const CbPairPlan& PP = b->plan.pairs;
+    if (e == cudaSuccess) e = upload(&b->d_ppasses, PP.passes);
+    if (e == cudaSuccess) e = upload(&b->d_pops, PP.ops);
+    if (e == cudaSuccess) e = upload(&b->d_playouts, PP.layouts);
+    if (e == cudaSuccess) e = upload(&b->d_pgates, PP.gates);
+    if (e == cudaSuccess) e = upload(&b->d_pitems, PP.items);
+    if (e == cudaSuccess) e = upload(&b->d_pphase_off, PP.phase_off);
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_ops, std::max<size_t>(1, b->plan.ops.size()) * sizeof(CbOp));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_pgates, std::max<size_t>(1, PP.gates.size()) * sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_energy, std::max<size_t>(1, b->n_circ) * sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_err, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_err, 4 * sizeof(unsigned));
     if (e != cudaSuccess) return fail("allocation", e);
     if (!b->plan.ops.empty()) std::memcpy(b->h_ops, b->plan.ops.data(), b->plan.ops.size() * sizeof(CbOp));
+    if (!PP.gates.empty()) std::memcpy(b->h_pgates, PP.gates.data(), PP.gates.size() * sizeof(double));
     b->smem = sizeof(CbPass) + (amp << MB);
     const void* fn = b->precision == SVB_FP64 ? (const void*)k_cbatch<double> : (const void*)k_cbatch<float>;
     int per_sm = 0, sms = 0;
@@ -577,6 +785,21 @@ svb_status cb_create_with(svb_circuit_batch* proto, int MB, int threads, svb_cir
         return m;
     }();
     b->grid = (unsigned)std::min<uint64_t>((uint64_t)per_sm * sms, std::max<uint64_t>(most, (uint64_t)sms));
+    if (PP.circuits > 0) {
+        // the pair launch: two CTAs of 256 threads per SM, the tile and the largest pass's data
+        b->psmem = (sizeof(double2) << PR_TILE_BITS) + PP.stage_bytes;
+        int pper = 0;
+        e = b->psmem <= PR_SMEM_CAP ? cudaFuncSetAttribute((const void*)k_cb_pairs,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PR_SMEM_CAP)
+                                    : cudaErrorInvalidValue;
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pper, (const void*)k_cb_pairs, PR_THREADS, b->psmem);
+        if (e != cudaSuccess || pper < 1) return fail("pair kernel setup", e);
+        uint64_t pmost = 1;
+        for (size_t p = 0; p + 1 < PP.phase_off.size(); p++)
+            pmost = std::max<uint64_t>(pmost, PP.phase_off[p + 1] - PP.phase_off[p]);
+        b->pgrid = (unsigned)std::min<uint64_t>((uint64_t)pper * sms, pmost);
+    }
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", e);
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
@@ -595,20 +818,20 @@ svb_status cb_create_with(svb_circuit_batch* proto, int MB, int threads, svb_cir
 
 svb_status cb_run(svb_circuit_batch* b)
 {
-    *b->h_err = 0;
+    std::memset(b->h_err, 0, 4 * sizeof(unsigned));
     cudaError_t e = b->graphed ? cudaGraphLaunch(b->graph, b->stream) : cb_enqueue(b, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return cb_cuda_fail(e, "svb_cbatch_run");
-    if (*b->h_err) {
+    if (b->h_err[1] | b->h_err[3]) {
         set_error("svb_cbatch_run: a grid barrier timed out; results are invalid");
         return SVB_ERR_STATE;
     }
     return SVB_OK;
 }
 
-// Autotuner cache: batch signature -> (tile bits, threads).
+// Autotuner cache: batch signature -> (tile bits, threads, pair engine).
 std::mutex g_tune_mutex;
-std::map<std::vector<uint64_t>, std::pair<int, int>> g_tune_cache;
+std::map<std::vector<uint64_t>, std::tuple<int, int, bool>> g_tune_cache;
 
 std::vector<uint64_t> signature(const svb_circuit_batch* b)
 {
@@ -637,8 +860,9 @@ svb_status svb_cbatch_create(int device, int precision, uint32_t n_circuits, con
     if (precision != SVB_FP64 && precision != SVB_FP32) return cb_invalid("svb_cbatch_create: bad precision");
     if (n_circuits == 0) return cb_invalid("svb_cbatch_create: no circuits");
     const int max_tb = precision == SVB_FP64 ? 12 : 13;
-    if (tile_bits != 0 && (tile_bits < 6 || tile_bits > max_tb))
-        return cb_invalid("svb_cbatch_create: tile_bits must be 0 (tune) or in [6, " + std::to_string(max_tb) + "]");
+    if (tile_bits != 0 && tile_bits != SVB_CBATCH_PAIRS && (tile_bits < 6 || tile_bits > max_tb))
+        return cb_invalid("svb_cbatch_create: tile_bits must be 0 (tune), SVB_CBATCH_PAIRS or in [6, " +
+                          std::to_string(max_tb) + "]");
     svb_circuit_batch proto;
     proto.device = device;
     proto.precision = precision;
@@ -670,7 +894,8 @@ svb_status svb_cbatch_create(int device, int precision, uint32_t n_circuits, con
     }
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return cb_cuda_fail(e, "svb_cbatch_create");
-    if (tile_bits != 0) return cb_create_with(&proto, tile_bits, 512, out);
+    if (tile_bits == SVB_CBATCH_PAIRS) return cb_create_with(&proto, max_tb, 512, true, out);
+    if (tile_bits != 0) return cb_create_with(&proto, tile_bits, 512, false, out);
 
     // autotune: the cached choice for this signature, else time the candidates
     const std::vector<uint64_t> sig = signature(&proto);
@@ -678,32 +903,42 @@ svb_status svb_cbatch_create(int device, int precision, uint32_t n_circuits, con
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(sig);
         if (it != g_tune_cache.end()) {
-            svb_status st = cb_create_with(&proto, it->second.first, it->second.second, out);
+            svb_status st = cb_create_with(&proto, std::get<0>(it->second), std::get<1>(it->second),
+                                           std::get<2>(it->second), out);
             if (st == SVB_OK) (*out)->tuned = true;
             return st;
         }
     }
+    // candidates: the sweep at three tile sizes and two block sizes, and (FP64, when a
+    // circuit has 12 or more qubits) the pair engine with the sweep's largest tile for the rest
+    std::vector<std::tuple<int, int, bool>> cands;
+    for (int tb = max_tb - 2; tb <= max_tb; tb++)
+        for (int threads : {256, 512}) cands.emplace_back(tb, threads, false);
+    if (precision == SVB_FP64 && max_n >= (uint32_t)PR_TILE_BITS) cands.emplace_back(max_tb, 512, true);
     svb_circuit_batch* best = nullptr;
     double best_ms = 0;
-    for (int tb = max_tb - 2; tb <= max_tb; tb++) {
-        for (int threads : {256, 512}) {
-            svb_circuit_batch* cand = nullptr;
-            if (cb_create_with(&proto, tb, threads, &cand) != SVB_OK) continue;
-            double ms = 1e300;
-            bool ok = cb_run(cand) == SVB_OK;           // warm-up
-            for (int r = 0; ok && r < 3; r++) {
-                const auto t0 = std::chrono::steady_clock::now();
-                ok = cb_run(cand) == SVB_OK;
-                const auto t1 = std::chrono::steady_clock::now();
-                ms = std::min(ms, std::chrono::duration<double, std::milli>(t1 - t0).count());
-            }
-            if (ok && (!best || ms < best_ms)) {
-                if (best) cb_free(best);
-                best = cand;
-                best_ms = ms;
-            } else {
-                cb_free(cand);
-            }
+    for (const auto& cfg : cands) {
+        const int tb = std::get<0>(cfg), threads = std::get<1>(cfg);
+        svb_circuit_batch* cand = nullptr;
+        if (cb_create_with(&proto, tb, threads, std::get<2>(cfg), &cand) != SVB_OK) continue;
+        if (std::get<2>(cfg) && cand->plan.pairs.circuits == 0) {      // nothing for the pair engine
+            cb_free(cand);
+            continue;
+        }
+        double ms = 1e300;
+        bool ok = cb_run(cand) == SVB_OK;           // warm-up
+        for (int r = 0; ok && r < 3; r++) {
+            const auto t0 = std::chrono::steady_clock::now();
+            ok = cb_run(cand) == SVB_OK;
+            const auto t1 = std::chrono::steady_clock::now();
+            ms = std::min(ms, std::chrono::duration<double, std::milli>(t1 - t0).count());
+        }
+        if (ok && (!best || ms < best_ms)) {
+            if (best) cb_free(best);
+            best = cand;
+            best_ms = ms;
+        } else {
+            cb_free(cand);
         }
     }
     if (!best) {
@@ -713,7 +948,7 @@ svb_status svb_cbatch_create(int device, int precision, uint32_t n_circuits, con
     best->tuned = true;
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
-        g_tune_cache[sig] = {best->tile_bits, best->threads};
+        g_tune_cache[sig] = std::make_tuple(best->tile_bits, best->threads, best->use_pairs);
     }
     *out = best;
     return SVB_OK;
@@ -731,13 +966,23 @@ svb_status svb_cbatch_run(svb_circuit_batch* b, const svb_gate* gates, double* e
                 return cb_invalid("svb_cbatch_run: gate " + std::to_string(g) + " differs from the batch's structure");
         CbPlan plan;
         std::string err;
-        if (!cb_build_plan(b, gates, b->tile_bits, plan, err)) return cb_invalid("svb_cbatch_run: " + err);
+        if (!cb_build_plan(b, gates, b->tile_bits, b->use_pairs, plan, err)) return cb_invalid("svb_cbatch_run: " + err);
         if (plan.ops.size() != b->plan.ops.size()) return cb_invalid("svb_cbatch_run: the plan's structure changed");
         for (size_t i = 0; i < plan.ops.size(); i++)
             if (plan.ops[i].form != b->plan.ops[i].form || plan.ops[i].p != b->plan.ops[i].p ||
                 plan.ops[i].flags != b->plan.ops[i].flags)
                 return cb_invalid("svb_cbatch_run: the plan's structure changed");
+        // the pair part: the same passes, ops and layouts, new gate fragments
+        const CbPairPlan &np = plan.pairs, &op = b->plan.pairs;
+        if (np.circuits != op.circuits || np.passes.size() != op.passes.size() || np.ops.size() != op.ops.size() ||
+            np.layouts.size() != op.layouts.size() || np.gates.size() != op.gates.size() ||
+            (!np.passes.empty() && std::memcmp(np.passes.data(), op.passes.data(), np.passes.size() * sizeof(PairPass))) ||
+            (!np.ops.empty() && std::memcmp(np.ops.data(), op.ops.data(), np.ops.size() * sizeof(PairOp))) ||
+            (!np.layouts.empty() && std::memcmp(np.layouts.data(), op.layouts.data(), np.layouts.size() * sizeof(DevStage))))
+            return cb_invalid("svb_cbatch_run: the plan's structure changed");
         std::memcpy(b->h_ops, plan.ops.data(), plan.ops.size() * sizeof(CbOp));
+        if (!np.gates.empty()) std::memcpy(b->h_pgates, np.gates.data(), np.gates.size() * sizeof(double));
+        b->plan.pairs.gates = np.gates;
         std::copy(gates, gates + b->gate_off[b->n_circ], b->gates.begin());
     }
     svb_status st = cb_run(b);
@@ -786,6 +1031,12 @@ svb_status svb_cbatch_info(const svb_circuit_batch* b, svb_cbatch_stats* out)
     out->moved_bytes = b->plan.moved_bytes;
     out->tuned = b->tuned ? 1u : 0u;
     out->n_passes = (uint32_t)b->plan.passes.size();
+    out->pair_circuits = b->plan.pairs.circuits;
+    out->pair_passes = (uint32_t)b->plan.pairs.passes.size();
+    out->pair_phases = (uint32_t)b->plan.pairs.phase_off.size() - 1;
+    out->pair_grid = b->pgrid;
+    out->n_phases = std::max(out->n_phases, out->pair_phases);
+    out->items += b->plan.pairs.items.size();
     return SVB_OK;
 }
 

@@ -55,7 +55,9 @@ class CbatchStats(ctypes.Structure):
                 ("pool_amplitudes", ctypes.c_uint64), ("items", ctypes.c_uint64),
                 ("grid", ctypes.c_uint32), ("graphed", ctypes.c_uint32),
                 ("moved_bytes", ctypes.c_double), ("tuned", ctypes.c_uint32),
-                ("n_passes", ctypes.c_uint32)]
+                ("n_passes", ctypes.c_uint32), ("pair_circuits", ctypes.c_uint32),
+                ("pair_passes", ctypes.c_uint32), ("pair_phases", ctypes.c_uint32),
+                ("pair_grid", ctypes.c_uint32)]
 
 
 _lib = None
@@ -347,10 +349,15 @@ class QaoaBatch:
         return st
 
 
+CBATCH_PAIRS = -1   # svb_cbatch_create: the pair engine where it can run
+
+
 class CircuitBatch:
     """Many independent circuits (each its own qubit count, 1..24) run together by one
     persistent, graph-replayed launch (svb_cbatch_*), with an optional Pauli-sum energy per
-    circuit.  tile_bits=0 lets the autotuner choose the tile and block sizes."""
+    circuit.  tile_bits=0 lets the autotuner choose the tile and block sizes and whether the
+    pair engine runs the FP64 circuits of 12 or more qubits; CBATCH_PAIRS asks for the pair
+    engine; 6..13 for shared-memory sweeps of that tile size."""
 
     def __init__(self, circuits, terms=None, device: int = 0, precision: int = SVB_FP64, tile_bits: int = 0):
         """circuits: list of (n_qubits, gate record array); terms: None or a list (one per

@@ -1,6 +1,7 @@
 """Batched circuits (svb_cbatch_*): circuits of uneven qubit counts run together by one
-persistent, graph-replayed launch, each checked against the oracle (state and Pauli-sum
-energy), with the tile and block sizes chosen by the autotuner or given."""
+persistent, graph-replayed launch (two with the pair engine), each checked against the
+oracle (state and Pauli-sum energy), with the tile and block sizes and the engine chosen by
+the autotuner or given."""
 import numpy as np
 import pytest
 
@@ -29,15 +30,21 @@ def mixed_batch(seed=0, count=20, lo=10, hi=22):
     return out
 
 
-@pytest.mark.parametrize("precision,tile_bits", [(0, 0), (0, 10), (1, 0)])
+@pytest.mark.parametrize("precision,tile_bits", [(0, 0), (0, 10), (1, 0), (0, -1)])
 def test_mixed_batch_matches_oracle(oracle, precision, tile_bits):
+    """tile_bits -1 (CBATCH_PAIRS): the FP64 circuits of 12 or more qubits without SRN on
+    the pair engine, the others (n = 10, 11, and those with SRN) on the sweep."""
     nat = native()
-    batch = mixed_batch(seed=1 + precision + tile_bits)
+    batch = mixed_batch(seed=1 + precision + abs(tile_bits))
     terms = [circuits.zz_x_hamiltonian(n) for n, _ in batch]
     terms[2] = None                          # a circuit without an observable
     b = nat.CircuitBatch(batch, terms, precision=precision, tile_bits=tile_bits)
     info = b.info()
     assert info.tuned == (1 if tile_bits == 0 else 0)
+    if tile_bits == nat.CBATCH_PAIRS:
+        eligible = sum(1 for i, (n, g) in enumerate(batch) if n >= 12 and i % 3 != 0)
+        assert info.pair_circuits == eligible and 0 < eligible < len(batch)
+        assert info.pair_phases > 0 and info.pair_grid > 0
     e = b.run()
     e2 = b.run()
     assert np.array_equal(e, e2)             # fixed-order sums: repeatable
@@ -69,15 +76,19 @@ def test_small_circuits_and_single_tiles(oracle):
     b.close()
 
 
-def test_parameter_sets_with_new_angles(oracle):
+@pytest.mark.parametrize("tile_bits", [0, -1])
+def test_parameter_sets_with_new_angles(oracle, tile_bits):
     """64 parameter points of one ansatz in one launch; new angles for the same structure
-    through svb_cbatch_run(gates), against the oracle's energies."""
+    through svb_cbatch_run(gates) (on the pair engine: new gate fragments for the same
+    blocks), against the oracle's energies."""
     nat = native()
     pc = circuits.hardware_efficient_ansatz(n=12, layers=4, seed=2)
     terms = circuits.zz_x_hamiltonian(pc.n)
     pts = np.random.default_rng(4).uniform(-np.pi, np.pi, size=(64, len(pc.params)))
     batch = [(pc.n, pc.evaluated(p)) for p in pts]
-    b = nat.CircuitBatch(batch, [terms] * len(batch))
+    b = nat.CircuitBatch(batch, [terms] * len(batch), tile_bits=tile_bits)
+    if tile_bits == nat.CBATCH_PAIRS:
+        assert b.info().pair_circuits == 64
     e = b.run()
     for i in (0, 17, 63):
         re, im = oracle.run(pc.n, batch[i][1])
