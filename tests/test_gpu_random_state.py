@@ -122,3 +122,40 @@ def test_batched_pairs_on_segments(oracle):
         re, im = oracle.run(nn, g)
         assert np.max(np.abs(b.state(i) - (re + 1j * im))) <= 1e-12, i
     b.close()
+
+
+def every_op_circuit(n, reps, seed, srn):
+    """All 38 ops of the reference, shuffled, on random qubits (SRN and the non-unitary R
+    only where asked: the pair engine takes matrices only)."""
+    import math
+    rng = np.random.default_rng(seed)
+    gl = []
+    for _ in range(reps):
+        names = list(G.OP_NAMES)
+        rng.shuffle(names)
+        for name in names:
+            if name == "SRN" and not srn:
+                continue
+            qs = [int(x) for x in rng.permutation(n)[:G.N_QUBITS[name]]]
+            npar = {"U3": 3, "U2": 2, "CU3": 3}.get(name, 1 if name in (
+                "U1", "RX", "RY", "RZ", "CRX", "CRY", "CRZ", "CU1", "RXX", "RZZ", "RYY", "R") else 0)
+            gl.append(G.FACTORIES[name](*([rng.uniform(-math.pi, math.pi) for _ in range(npar)] + qs)))
+    return G.to_array(gl)
+
+
+@pytest.mark.parametrize("n,seed", [(12, 1), (15, 2), (17, 3), (21, 4)])
+def test_every_op_every_engine_on_random_state(oracle, n, seed):
+    """Differential check: every op, every FP64 engine, a random input state, the oracle."""
+    from svsim_b200 import _native as nat
+    g = every_op_circuit(n, 3, seed, srn=False)
+    st = random_state(n, 300 + seed)
+    ore, oim = oracle.run(n, g, state=st)
+    want = ore + 1j * oim
+    for engine, tile in ((nat.ENGINE_PAIRS, 0), (nat.ENGINE_STAGED, 10), (nat.ENGINE_STAGED, 11),
+                         (nat.ENGINE_STAGED, 12), (nat.ENGINE_PER_GATE, 0)):
+        got = run_on(nat, n, g, st, nat.SVB_FP64, engine, tile)
+        assert np.max(np.abs(got - want)) <= 1e-12, (engine, tile)
+    for k in (4, 5, 6):
+        got = run_on(nat, n, g, st, nat.SVB_FP32, nat.ENGINE_FUSED, 0, k)
+        f = abs(np.vdot(want, got)) ** 2 / (np.vdot(got, got).real * np.vdot(want, want).real)
+        assert 1 - f <= 1e-6, k
