@@ -100,6 +100,9 @@ bool fusable(const std::vector<EOp>& ops)
     return true;
 }
 
+// seeds tried per block (the first remaining ops that can move to the front)
+constexpr size_t kSeedWindow = 8;
+
 void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
 {
     plan = FusedPlan{};
@@ -161,20 +164,40 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
         struct BlockOps { std::vector<int> tq; std::vector<int> ops; };
         std::vector<BlockOps> pblocks;
         remaining = taken;
-        while (!remaining.empty() && (int)pblocks.size() < fused_max_blocks(k)) {
-            uint64_t S = 0;
-            uint64_t blk_blocked = 0;
-            blk.clear();
-            rest.clear();
+        // A block is grown in program order from a seed set of qubits: an op joins while
+        // the union stays within k qubits and none of its qubits is held by an op left
+        // out before it.  Seeds: the first remaining op, and each of the next ones that
+        // could move to the front (no earlier remaining op shares a qubit); the seed whose
+        // block takes the most ops is kept (n=30: 227 -> 219 blocks at k = 5).
+        auto grow = [&](uint64_t S0, std::vector<int>& b, std::vector<int>& r) {
+            uint64_t S = S0, held = 0;
+            b.clear();
+            r.clear();
             for (int i : remaining) {
                 const uint64_t t = op_qubits(ops[i]);
-                if (t & blk_blocked) { blk_blocked |= t; rest.push_back(i); continue; }
-                if (__builtin_popcountll(S | t) <= k) {
+                if (!(t & held) && __builtin_popcountll(S | t) <= k) {
                     S |= t;
-                    blk.push_back(i);
+                    b.push_back(i);
                 } else {
-                    blk_blocked |= t;
-                    rest.push_back(i);
+                    held |= t;
+                    r.push_back(i);
+                }
+            }
+            return S;
+        };
+        std::vector<int> blk2, rest2;
+        while (!remaining.empty() && (int)pblocks.size() < fused_max_blocks(k)) {
+            uint64_t S = grow(0, blk, rest);
+            uint64_t front = op_qubits(ops[remaining[0]]);
+            for (size_t c = 1; c < remaining.size() && c < kSeedWindow; c++) {
+                const uint64_t t = op_qubits(ops[remaining[c]]);
+                if (t & front) { front |= t; continue; }
+                front |= t;
+                const uint64_t S2 = grow(t, blk2, rest2);
+                if (blk2.size() > blk.size()) {
+                    blk.swap(blk2);
+                    rest.swap(rest2);
+                    S = S2;
                 }
             }
             // targets: the block's qubits, padded with other local qubits to exactly k
@@ -410,20 +433,43 @@ void plan_fused6(const std::vector<EOp>& ops, int n, FusedPlan& plan)
     for (;;) {
         while (first < N_ops && done[first]) first++;
         if (first == N_ops) break;
-        uint64_t S = 0, blocked = 0;
-        blk.clear();
-        for (size_t i = first; i < N_ops; i++) {
-            if (done[i]) continue;
-            const uint64_t t = op_qubits(ops[i]);
-            if ((t & blocked) || __builtin_popcountll(S | t) > F6_K) {
-                blocked |= t;
-                if (blocked == all) break;
-                continue;
+        // the block grown from a seed set (as in plan_fused), best of the front-movable seeds
+        auto grow6 = [&](uint64_t S0, std::vector<int>& b) {
+            uint64_t S = S0, blocked = 0;
+            b.clear();
+            for (size_t i = first; i < N_ops; i++) {
+                if (done[i]) continue;
+                const uint64_t t = op_qubits(ops[i]);
+                if ((t & blocked) || __builtin_popcountll(S | t) > F6_K) {
+                    blocked |= t;
+                    if (blocked == all) break;
+                    continue;
+                }
+                S |= t;
+                b.push_back((int)i);
             }
-            S |= t;
-            blk.push_back((int)i);
-            done[i] = 1;
+            return S;
+        };
+        uint64_t S = grow6(0, blk);
+        {
+            std::vector<int> blk2;
+            uint64_t front = 0;
+            size_t seen = 0;
+            for (size_t i = first; i < N_ops && seen < kSeedWindow; i++) {
+                if (done[i]) continue;
+                seen++;
+                const uint64_t t = op_qubits(ops[i]);
+                if (t & front) { front |= t; continue; }
+                front |= t;
+                if (seen == 1) continue;
+                const uint64_t S2 = grow6(t, blk2);
+                if (blk2.size() > blk.size()) {
+                    blk.swap(blk2);
+                    S = S2;
+                }
+            }
         }
+        for (int i : blk) done[i] = 1;
         // targets: the block's qubits, padded from the top; rows: the 6 lowest others
         uint64_t T = S;
         for (int q = n - 1; q >= 0 && __builtin_popcountll(T) < F6_K; q--) T |= bit(q);
