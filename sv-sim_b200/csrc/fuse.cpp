@@ -100,8 +100,11 @@ bool fusable(const std::vector<EOp>& ops)
     return true;
 }
 
-// seeds tried per block (the first remaining ops that can move to the front)
-constexpr size_t kSeedWindow = 8;
+// seeds tried per block (the first open ops that can move to the front); fewer for the
+// six-qubit blocks, whose passes are many (n = 30: 148 passes with 8 seeds, 146 with 32 at
+// four times the planning time)
+constexpr size_t kSeedWindow = 32;
+constexpr size_t kSeedWindow6 = 8;
 
 void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
 {
@@ -113,27 +116,72 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
     const uint64_t all = (n >= 64) ? ~0ull : (bit(n) - 1);
     std::vector<char> done(N_ops, 0);
     size_t first = 0;
-    std::vector<int> taken, remaining, rest, blk;
+    std::vector<int> remaining, rest, blk;
     for (;;) {
         while (first < N_ops && done[first]) first++;
         if (first == N_ops) break;
-        // -- local qubits of the pass: every qubit of an op must be local
+        // -- the pass's blocks first, then its local qubits.  A block grows in program
+        // order from a seed set of qubits over every op not yet placed: an op joins while
+        // the block stays within k qubits, the pass within M local qubits (the G lowest
+        // always among them), and none of its qubits is held by an op left out before it
+        // (so the ops left out commute past the block).  Seeds: the first open op and each
+        // of the next ones that could move to the front (no earlier open op shares a
+        // qubit); the block that takes the most ops is kept.  Up to fused_max_blocks(k)
+        // blocks per pass; the pass's local qubits are their union, padded from the lowest.
+        // (n = 30, k = 5: 69 passes and 186 blocks, against 81 and 227 for a pass cut in
+        // program order with blocks grown from the first op.)
         uint64_t L = (n == M) ? all : (bit(G) - 1);
-        int nL = (n == M) ? n : G;
-        uint64_t blocked = 0;
-        taken.clear();
-        for (size_t i = first; i < N_ops; i++) {
-            if (done[i]) continue;
-            const uint64_t t = op_qubits(ops[i]);
-            if (t & blocked) { blocked |= t; if (blocked == all) break; continue; }
-            const uint64_t need = t & ~L;
-            const int add = __builtin_popcountll(need);
-            if (nL + add > M) { blocked |= t; if (blocked == all) break; continue; }
-            L |= need;
-            nL += add;
-            taken.push_back((int)i);
-            done[i] = 1;
+        remaining.clear();
+        for (size_t i = first; i < N_ops; i++)
+            if (!done[i]) remaining.push_back((int)i);
+        struct Grown { uint64_t S; std::vector<int> ops; };
+        std::vector<Grown> grown;
+        auto grow = [&](uint64_t S0, std::vector<int>& b, std::vector<int>& r) {
+            uint64_t S = S0, held = 0;
+            b.clear();
+            r.clear();
+            for (size_t x = 0; x < remaining.size(); x++) {
+                const int i = remaining[x];
+                const uint64_t t = op_qubits(ops[i]);
+                if (!(t & held) && __builtin_popcountll(S | t) <= k && __builtin_popcountll(L | S | t) <= M) {
+                    S |= t;
+                    b.push_back(i);
+                } else {
+                    held |= t;
+                    r.push_back(i);
+                    if (held == all) {               // nothing later can join
+                        r.insert(r.end(), remaining.begin() + (long)x + 1, remaining.end());
+                        break;
+                    }
+                }
+            }
+            return S;
+        };
+        {
+            std::vector<int> b2, r2;
+            while ((int)grown.size() < fused_max_blocks(k) && !remaining.empty()) {
+                uint64_t S = grow(0, blk, rest);
+                uint64_t front = op_qubits(ops[remaining[0]]);
+                for (size_t c = 1; c < remaining.size() && c < kSeedWindow; c++) {
+                    const uint64_t t = op_qubits(ops[remaining[c]]);
+                    if (t & front) { front |= t; continue; }
+                    front |= t;
+                    if (__builtin_popcountll(L | t) > M) continue;
+                    const uint64_t S2 = grow(t, b2, r2);
+                    if (b2.size() > blk.size()) {
+                        blk.swap(b2);
+                        rest.swap(r2);
+                        S = S2;
+                    }
+                }
+                if (blk.empty()) break;
+                L |= S;
+                for (int i : blk) done[i] = 1;
+                grown.push_back({S, blk});
+                remaining.swap(rest);
+            }
         }
+        int nL = __builtin_popcountll(L);
         for (int q = 0; nL < M && q < n; q++)
             if (!((L >> q) & 1)) { L |= bit(q); nL++; }
 
@@ -160,47 +208,11 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
         }
         P.block_begin = (int32_t)plan.blocks.size();
 
-        // -- blocks: up to k qubits each, commuting ops pulled forward
+        // -- the blocks' targets: their qubits, padded with other local qubits to exactly k
         struct BlockOps { std::vector<int> tq; std::vector<int> ops; };
         std::vector<BlockOps> pblocks;
-        remaining = taken;
-        // A block is grown in program order from a seed set of qubits: an op joins while
-        // the union stays within k qubits and none of its qubits is held by an op left
-        // out before it.  Seeds: the first remaining op, and each of the next ones that
-        // could move to the front (no earlier remaining op shares a qubit); the seed whose
-        // block takes the most ops is kept (n=30: 227 -> 219 blocks at k = 5).
-        auto grow = [&](uint64_t S0, std::vector<int>& b, std::vector<int>& r) {
-            uint64_t S = S0, held = 0;
-            b.clear();
-            r.clear();
-            for (int i : remaining) {
-                const uint64_t t = op_qubits(ops[i]);
-                if (!(t & held) && __builtin_popcountll(S | t) <= k) {
-                    S |= t;
-                    b.push_back(i);
-                } else {
-                    held |= t;
-                    r.push_back(i);
-                }
-            }
-            return S;
-        };
-        std::vector<int> blk2, rest2;
-        while (!remaining.empty() && (int)pblocks.size() < fused_max_blocks(k)) {
-            uint64_t S = grow(0, blk, rest);
-            uint64_t front = op_qubits(ops[remaining[0]]);
-            for (size_t c = 1; c < remaining.size() && c < kSeedWindow; c++) {
-                const uint64_t t = op_qubits(ops[remaining[c]]);
-                if (t & front) { front |= t; continue; }
-                front |= t;
-                const uint64_t S2 = grow(t, blk2, rest2);
-                if (blk2.size() > blk.size()) {
-                    blk.swap(blk2);
-                    rest.swap(rest2);
-                    S = S2;
-                }
-            }
-            // targets: the block's qubits, padded with other local qubits to exactly k
+        for (const Grown& gb : grown) {
+            uint64_t S = gb.S;
             std::vector<int> tq;
             for (int q = 0; q < n; q++)
                 if ((S >> q) & 1) tq.push_back(q);
@@ -208,8 +220,7 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
                 const int q = P.local_q[p];
                 if (!((S >> q) & 1)) { tq.push_back(q); S |= bit(q); }
             }
-            pblocks.push_back({tq, blk});
-            remaining.swap(rest);
+            pblocks.push_back({tq, gb.ops});
         }
         const int nblocks = (int)pblocks.size();
 
@@ -377,7 +388,6 @@ void plan_fused(const std::vector<EOp>& ops, int n, int k, FusedPlan& plan)
             }
             plan.blocks.push_back(B);
         }
-        for (int i : remaining) done[i] = 0;   // did not fit in this pass's blocks
         P.n_blocks = nblocks;
         plan.passes.push_back(P);
     }
@@ -455,7 +465,7 @@ void plan_fused6(const std::vector<EOp>& ops, int n, FusedPlan& plan)
             std::vector<int> blk2;
             uint64_t front = 0;
             size_t seen = 0;
-            for (size_t i = first; i < N_ops && seen < kSeedWindow; i++) {
+            for (size_t i = first; i < N_ops && seen < kSeedWindow6; i++) {
                 if (done[i]) continue;
                 seen++;
                 const uint64_t t = op_qubits(ops[i]);
