@@ -139,3 +139,27 @@ def test_autotune_single_circuit(oracle, n, precision):
     else:
         assert 1 - abs(np.vdot(b, a)) ** 2 / (np.vdot(a, a).real * np.vdot(b, b).real) <= 1e-6
     h.close()
+
+
+def test_pair_engine_request_on_fp32_and_small_circuits(oracle):
+    """CBATCH_PAIRS where the pair engine cannot run (FP32, n < 12, SRN) keeps every circuit
+    on the shared-memory sweep, with the same results."""
+    nat = native()
+    batch = [(n, circuits.random_matching_circuit(n, 4, seed=40 + n)) for n in (8, 11, 13)]
+    b = nat.CircuitBatch(batch, precision=1, tile_bits=nat.CBATCH_PAIRS)
+    assert b.info().pair_circuits == 0
+    b.run()
+    for i, (n, g) in enumerate(batch):
+        re, im = oracle.run(n, g)
+        a = b.state(i)
+        ref = re + 1j * im
+        f = abs(np.vdot(ref, a)) ** 2 / (np.vdot(a, a).real * np.vdot(ref, ref).real)
+        assert 1 - f <= 1e-6, n
+    b.close()
+    srn = [(13, np.concatenate([circuits.random_matching_circuit(13, 3, seed=7), G.to_array([G.SRN(2)])]))]
+    b = nat.CircuitBatch(srn, tile_bits=nat.CBATCH_PAIRS)
+    assert b.info().pair_circuits == 0
+    b.run()
+    re, im = oracle.run(13, srn[0][1])
+    assert np.max(np.abs(b.state(0) - (re + 1j * im))) <= 1e-12
+    b.close()
