@@ -214,7 +214,8 @@ struct PassBuilder {
 }  // namespace
 
 void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
-                   const std::function<std::vector<int>(uint64_t, const std::vector<int>&)>& build)
+                   const std::function<std::vector<int>(uint64_t, const std::vector<int>&)>& build,
+                   int seeds)
 {
     const size_t N = ops.size();
     const uint64_t all = (n >= 64) ? ~0ull : (bit(n) - 1);
@@ -228,10 +229,16 @@ void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
         int nL = 0;
         std::vector<int> taken, entries;   // entries: taken ops that made qubits local
     };
-    // one greedy scan from `first` in program order; op `banned` is treated as blocked
-    auto scan = [&](long banned, Cut& c) {
+    // one greedy scan from `first` in program order; op `banned` is treated as blocked;
+    // op `seed` (if any) makes its qubits local first
+    auto scan = [&](long banned, Cut& c, long seed = -1) {
         c.L = (n == M) ? all : low;
         c.nL = (n == M) ? n : G;
+        if (seed >= 0) {
+            const int q = inf[seed].need, q2 = inf[seed].need2;
+            if (q >= 0 && !((c.L >> q) & 1)) { c.L |= bit(q); c.nL++; }
+            if (q2 >= 0 && !((c.L >> q2) & 1)) { c.L |= bit(q2); c.nL++; }
+        }
         c.taken.clear();
         c.entries.clear();
         uint64_t blocked = 0;
@@ -266,6 +273,18 @@ void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
         while (first < N && done[first]) first++;
         if (first == N) break;
         scan(-1, best);
+        uint64_t front = 0;
+        int seen = 0;
+        for (size_t i = first; i < N && seen < seeds; i++) {
+            if (done[i]) continue;
+            seen++;
+            const uint64_t t = inf[i].touch;
+            if (t & front) { front |= t; continue; }
+            front |= t;
+            if (seen == 1) continue;
+            scan(-1, alt, (long)i);
+            if (alt.taken.size() > best.taken.size()) std::swap(best, alt);
+        }
         // one step of local search: leaving out one of the ops that chose the local
         // qubits (the first op excepted, so that every pass makes progress) may let the
         // pass take more ops

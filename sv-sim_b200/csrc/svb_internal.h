@@ -210,10 +210,13 @@ cudaError_t launch_pair_pass(void* state, int n, int pass_index, const DevPairBu
 // taken into a pass of M local qubits (always including the G lowest) while their dense
 // or CX target can be made local and they touch no qubit of an op skipped earlier; of the
 // cuts that leave out one of the ops that brought new qubits in, the one taking the most
-// ops is kept.  `build` receives each pass's local-qubit mask and ops and returns the ops
+// ops is kept.  With seeds > 1, each of the first `seeds` open ops that could move to the
+// front (no earlier open op shares a qubit) is also tried as the one that brings the first
+// new qubits in.  `build` receives each pass's local-qubit mask and ops and returns the ops
 // it could not place.
 void select_passes(const std::vector<EOp>& ops, int n, int M, int G,
-                   const std::function<std::vector<int>(uint64_t, const std::vector<int>&)>& build);
+                   const std::function<std::vector<int>(uint64_t, const std::vector<int>&)>& build,
+                   int seeds = 1);
 
 // ---------------------------------------------------------------------------------
 // Fused tensor-core engine (FP32 states): passes of up to FT_MAX_BLOCKS fused k-qubit
