@@ -861,7 +861,8 @@ extern "C" svb_status svb_adjoint(svb_sim* s, const svb_gate* gates, const svb_p
             const size_t e0 = c < ckpts.size() ? ckpt_at[c] : K;
             std::vector<EOp> seg(eops.begin() + b0, eops.begin() + e0);
             PairPlan P;
-            if (!plan_pairs(seg, n, P) || !append_pair_plan(fwd, P)) fwd_pairs = false;
+            // the program-order cut only: this planning is on every gradient's path
+            if (!plan_pairs(seg, n, P, nullptr, false) || !append_pair_plan(fwd, P)) fwd_pairs = false;
             seg_pass_end.push_back(fwd.passes.size());
             b0 = e0;
         }

@@ -721,9 +721,10 @@ double plan_cost(const PairPlan& p)
 // (select_passes with 32 seeds) give different plans; the cheaper by the cost model is
 // kept (n = 30: 48 passes and 529 blocks, 936 ms, against 50, 539 and 952 ms; at n = 26
 // the program-order cut is the cheaper).
-bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::vector<Mat4>* mats)
+bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::vector<Mat4>* mats, bool both_cuts)
 {
     if (!plan_pairs_cut(ops, n, plan, mats, 1)) return false;
+    if (!both_cuts) return true;
     PairPlan alt;
     if (plan_pairs_cut(ops, n, alt, mats, 32) && plan_cost(alt) < plan_cost(plan)) plan = std::move(alt);
     return true;

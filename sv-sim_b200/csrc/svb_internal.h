@@ -194,8 +194,11 @@ struct PairPlan {
 using Mat4 = std::array<double, 32>;
 
 // Builds the pair plan; false if an op cannot be written as a matrix (SRN).  `mats` holds
-// the matrices of F_M4 ops.
-bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::vector<Mat4>* mats = nullptr);
+// the matrices of F_M4 ops.  With both_cuts, the seeded pass cut is planned as well and the
+// cheaper plan kept (about twice the planning time; callers that plan on every call of a
+// short circuit, such as the adjoint's forward segments, plan the program-order cut only).
+bool plan_pairs(const std::vector<EOp>& ops, int n, PairPlan& plan, const std::vector<Mat4>* mats = nullptr,
+                bool both_cuts = true);
 
 struct DevPairBuffers {
     PairPass* passes = nullptr;
