@@ -531,13 +531,13 @@ extern "C" int emu_pairs_run_from(uint32_t n, const svb_gate* gates, size_t n_ga
     return pairs_run(n, gates, n_gates, re, im, stats, true);
 }
 
-extern "C" int emu_pairs_stats(uint32_t n, const svb_gate* gates, size_t n_gates, uint64_t* stats)
+static int pairs_stats(uint32_t n, const svb_gate* gates, size_t n_gates, uint64_t* stats, bool both_cuts)
 {
     std::vector<EOp> eops;
     for (size_t i = 0; i < n_gates; i++)
         if (!lower_gate(gates[i], (int32_t)i, eops)) return -1;
     PairPlan plan;
-    if (!plan_pairs(eops, (int)n, plan)) return -6;
+    if (!plan_pairs(eops, (int)n, plan, nullptr, both_cuts)) return -6;
     stats[0] = plan.passes.size();
     stats[1] = plan.n_blocks;
     stats[2] = plan.n_swaps;
@@ -550,6 +550,17 @@ extern "C" int emu_pairs_stats(uint32_t n, const svb_gate* gates, size_t n_gates
     stats[5] = plan.stage_bytes;
     stats[6] = plan.n_lane_perms;
     return 0;
+}
+
+extern "C" int emu_pairs_stats(uint32_t n, const svb_gate* gates, size_t n_gates, uint64_t* stats)
+{
+    return pairs_stats(n, gates, n_gates, stats, true);
+}
+
+// The same for the program-order pass cut alone.
+extern "C" int emu_pairs_stats_one_cut(uint32_t n, const svb_gate* gates, size_t n_gates, uint64_t* stats)
+{
+    return pairs_stats(n, gates, n_gates, stats, false);
 }
 
 // ---- shared-memory bank model of the fused kernel's accesses ---------------------------

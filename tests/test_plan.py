@@ -370,3 +370,25 @@ def test_fused_plans_on_random_state(emu, oracle, case):
                                     im.ctypes.data_as(_dp), ctypes.byref(a))
         assert rc == 0, k
         assert 1 - fidelity(re + 1j * im, ore + 1j * oim) < 1e-12, k
+
+
+def plan_cost(st):
+    """The pair planner's cost model, in block units: blocks + 0.49 exchanges + 0.36 lane
+    permutations + 2.05 relayouts + 0.6 passes."""
+    return int(st[1]) + 0.49 * int(st[2]) + 0.36 * int(st[6]) + 2.05 * int(st[3]) + 0.6 * int(st[0])
+
+
+@pytest.mark.parametrize("n,depth,seed", [(14, 12, 1), (18, 20, 2), (20, 40, 2024), (24, 40, 2024), (30, 40, 2024)])
+def test_pair_plan_keeps_the_cheaper_pass_cut(emu, n, depth, seed):
+    """plan_pairs plans the program-order and the seeded pass cut and keeps the cheaper by
+    the cost model: never above the program-order plan; at n = 30 the seeded one (48
+    passes against 50)."""
+    g = circuits.random_matching_circuit(n, depth, seed=seed)
+    both, one = np.zeros(8, dtype=np.uint64), np.zeros(8, dtype=np.uint64)
+    vp = ctypes.c_void_p
+    assert emu.emu_pairs_stats(ctypes.c_uint32(n), vp(g.ctypes.data), ctypes.c_size_t(len(g)), vp(both.ctypes.data)) == 0
+    assert emu.emu_pairs_stats_one_cut(ctypes.c_uint32(n), vp(g.ctypes.data), ctypes.c_size_t(len(g)),
+                                       vp(one.ctypes.data)) == 0
+    assert plan_cost(both) <= plan_cost(one) + 1e-9
+    if n == 30:
+        assert int(one[0]) == 50 and int(both[0]) == 48 and plan_cost(both) < plan_cost(one)
